@@ -1,0 +1,376 @@
+#!/usr/bin/env python3
+"""Benchmark of the Kohn-Sham H|psi> path on the B200 (and the reference CPU arm).
+
+Workload (one "step"): one application of H = V + V_NL - 1/2 Lap (8th-order FD)
+to a batch of 256 states of the 64-atom diamond cell on an 80^3 grid, FP64,
+states resident in HBM (1.05 GB of states in, 1.05 GB out: larger than L2, so
+no flush is needed between steps). ``value`` is algorithmic HBM GB/s of the
+whole apply:  bytes = N*ns*2*8 (read psi, write H psi) + N*8 (V)
+                    + n_atoms*4*n_sphere*8 (projector tables).
+``e2e`` is the same metric through the host-buffer C entry point
+(qg_hamiltonian_apply_host_d) with pinned host states: H2D + apply + D2H.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank applies H to its own 256 states on its own GPU
+(weak scaling, no data-path collective); ``value`` is the total over ranks
+divided by the max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NS = 256
+REPS = (2, 2, 2)
+FD_ORDER = 8
+WORKLOAD = "diamond64_80cube_Hpsi"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sweep", action="store_true", help="also time FD orders 2/4/6 and FP32")
+    return p.parse_args()
+
+
+def algorithmic_bytes(cell, ns, elem=8, n_sphere_pts=None):
+    N = cell.N
+    proj = (n_sphere_pts if n_sphere_pts is not None else 0) * 4 * elem
+    return N * ns * 2 * elem + N * elem + proj
+
+
+def sphere_points(cell):
+    """Projector points with a nonzero table value, summed over atoms."""
+    import numpy as np
+    tot = 0
+    for per_k in cell.cubes:
+        nz = None
+        for (_, _, w) in per_k:
+            m = w != 0.0
+            nz = m if nz is None else (nz | m)
+        tot += int(nz.sum()) if nz is not None else 0
+    return tot
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# --------------------------------------------------------------- CPU arms
+def _ref_worker(args):
+    """One single-thread process applying the reference H to a slice of states."""
+    reps, ns, seed, order = args
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    import numpy as np
+    import oracle as O
+    from qumasun_b200.cell import build_cell, initial_states
+    cell = build_cell(reps=reps, fd_order=order)
+    X = initial_states(ns, cell.N, seed=seed)
+    t0 = time.perf_counter()
+    O.hamiltonian_apply(cell, X, impl="ref" if O.ref_available() else "port")
+    return time.perf_counter() - t0
+
+
+def cpu_reference_rate(states_per_proc=2, procs=None, order=FD_ORDER):
+    """States/s of the reference CPU H-apply on the host cores: `procs` concurrent
+    single-thread processes on disjoint state slices (the reference runs one
+    state per OpeA call, single-threaded per rank)."""
+    import multiprocessing as mp
+    import oracle as O
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_ref_worker, [(REPS, states_per_proc, 100 + i, order) for i in range(procs)])
+    wall = time.perf_counter() - t0
+    per_state = max(times) / states_per_proc
+    kind = "reference" if O.ref_available() else "port"
+    return dict(states_per_s=procs / per_state, cores=procs, kind=kind,
+                sample=f"{procs} processes x {states_per_proc} states of the 80^3 64-atom cell, "
+                       f"FD order {order}, one thread each (max process time {max(times):.2f} s, wall {wall:.1f} s)")
+
+
+def run_reference_arm(a):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from qumasun_b200.cell import build_cell
+    cell = build_cell(reps=REPS)
+    nsph = sphere_points(cell)
+    per_state_bytes = algorithmic_bytes(cell, NS, n_sphere_pts=nsph) / NS
+    rates = []
+    for _ in range(a.warmup):
+        pass  # the CPU arm has no device warm-up; the first timed sample includes nothing to amortise
+    t_all = time.perf_counter()
+    for _ in range(max(1, a.steps)):
+        r = cpu_reference_rate(states_per_proc=1)
+        rates.append(r["states_per_s"])
+        if time.perf_counter() - t_all > 150:
+            break
+    sps = sorted(rates)[len(rates) // 2]
+    gbs = sps * per_state_bytes / 1e9
+    line = {
+        "metric": "H|psi> GB/s (algorithmic)", "value": round(gbs, 3), "unit": "GB/s",
+        "impl": "reference", "n_gpus": a.gpus, "steps": len(rates), "warmup": a.warmup,
+        "ms_per_step": round(NS / sps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_states": NS, "grid": [80, 80, 80], "atoms": 64,
+                   "fd_order": FD_ORDER},
+        "state_applications_per_s": round(sps, 3),
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": r["cores"],
+                         "kind": r["kind"], "sample": r["sample"]},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm
+def run_gpu_arm(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from qumasun_b200 import Context, Hamiltonian
+    from qumasun_b200.cell import build_cell
+
+    cell = build_cell(reps=REPS)
+    nsph = sphere_points(cell)
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    H = Hamiltonian(ctx, cell, fd_order=FD_ORDER)
+    N = cell.N
+    gen = torch.Generator(device="cuda").manual_seed(1000 + rank)
+    with torch.cuda.stream(stream):
+        X = torch.rand(NS, N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+        HX = torch.empty_like(X)
+    stream.synchronize()
+    nbytes = algorithmic_bytes(cell, NS, n_sphere_pts=nsph)
+    launches_per_step = H.launches_per_apply(NS)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    for _ in range(max(3, a.warmup)):
+        H.apply_device(NS, X.data_ptr(), HX.data_ptr())
+    stream.synchronize()
+
+    # timed region: device events on the launching stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            H.apply_device(NS, X.data_ptr(), HX.data_ptr())
+        e1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / a.steps
+    ms_max = max_over_ranks(ms)
+    gbs = nbytes * ws / (ms_max * 1e-3) / 1e9
+
+    # dominant-kernel roofline: per-phase device times of one apply
+    phases = [H.apply_timed(NS, X.data_ptr(), HX.data_ptr()) for _ in range(5)]
+    ms_proj = sorted(p[0] for p in phases)[2]
+    ms_sten = sorted(p[1] for p in phases)[2]
+    pj_pts = nsph
+    sten_bytes = N * NS * 2 * 8 + N * 8 + pj_pts * (4 * 8 + 4) + (N + 1) * 4
+    proj_bytes = pj_pts * (4 * 8 + 4) + pj_pts * NS * 8  # tables + gathered psi (upper bound, L2 may serve part)
+    peak, peak_kind = measured_peak_hbm()
+    sten_gbs = sten_bytes / (ms_sten * 1e-3) / 1e9
+
+    # e2e through the host-buffer entry point with pinned host states
+    Xh = torch.empty(NS, N, dtype=torch.float64, pin_memory=True)
+    Xh.copy_(X.cpu())
+    HXh = torch.empty_like(Xh).pin_memory()
+    e2e_steps = max(2, min(a.steps, 5))
+    H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())  # warm the staging buffers
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = max_over_ranks(e2e_s)
+    e2e_gbs = nbytes * ws / e2e_s / 1e9
+
+    sweep = {}
+    if a.sweep and rank == 0:
+        for order in (2, 4, 6, 8):
+            Ho = Hamiltonian(ctx, cell, fd_order=order)
+            for dt in ("f64", "f32"):
+                Xs = X if dt == "f64" else X.float()
+                HXs = torch.empty_like(Xs)
+                for _ in range(3):
+                    Ho.apply_device(NS, Xs.data_ptr(), HXs.data_ptr(), dtype=dt)
+                stream.synchronize()
+                s0 = torch.cuda.Event(enable_timing=True)
+                s1 = torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                for _ in range(5):
+                    Ho.apply_device(NS, Xs.data_ptr(), HXs.data_ptr(), dtype=dt)
+                s1.record(stream)
+                stream.synchronize()
+                m = s0.elapsed_time(s1) / 5
+                el = 8 if dt == "f64" else 4
+                sweep[f"o{order}_{dt}"] = {"ms": round(m, 4),
+                                           "GBs": round(algorithmic_bytes(cell, NS, el, nsph) / (m * 1e-3) / 1e9, 1),
+                                           "state_apps_per_s": round(NS / (m * 1e-3), 1)}
+                del Xs, HXs
+            Ho.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        try:
+            r = cpu_reference_rate(states_per_proc=1)
+            per_state = nbytes / NS
+            cpu = {"value": round(r["states_per_s"] * per_state / 1e9, 3), "unit": "GB/s", "cores": r["cores"],
+                   "kind": r["kind"], "sample": r["sample"],
+                   "state_applications_per_s": round(r["states_per_s"], 3)}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": "H|psi> GB/s (algorithmic)", "value": round(gbs, 2), "unit": "GB/s",
+            "n_gpus": ws, "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": round(ms_max, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_states": NS, "grid": [cell.nx, cell.ny, cell.nz],
+                       "atoms": cell.n_atoms, "fd_order": FD_ORDER, "parallelism": f"states-replicated x{ws}",
+                       "l2": "inputs larger than L2 (1.05 GB states), no flush"},
+            "state_applications_per_s": round(NS * ws / (ms_max * 1e-3), 1),
+            "roofline": {"bound": "hbm", "kernel": "k_hamiltonian (stencil+V+projector scatter)",
+                         "achieved": round(sten_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(sten_gbs / peak, 4), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": sten_bytes, "ms_per_launch": round(ms_sten, 4),
+                         "traffic": None,
+                         "k_project_ms": round(ms_proj, 4),
+                         "k_project_gbs_upper": round(proj_bytes / (ms_proj * 1e-3) / 1e9, 1)},
+            "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": NS * N * 8,
+                    "d2h_bytes_per_step": NS * N * 8, "seconds_per_step": round(e2e_s, 5)},
+            "gpu_launches": launches_per_step * a.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        if sweep:
+            line["sweep"] = sweep
+        print(json.dumps(line), flush=True)
+    H.close()
+    ctx.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    return run_gpu_arm(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,132 @@
+/*
+ * qumasun_b200.h -- C ABI of the B200 Kohn-Sham H|psi> + LOBPCG engine.
+ *
+ * Plain C: opaque handles, integer status returns, plain pointers and sizes.
+ * Every entry point returns QG_OK (0) or a negative qg_status. Nothing here
+ * falls back to the CPU: without a usable CUDA device every call that needs
+ * one returns QG_ERR_CUDA.
+ *
+ * Layout contract (same as the reference, so its buffers copy in without a
+ * transpose): one state is an x-fastest grid array, index ix + nx*(iy + ny*iz);
+ * a block of states is state-major, state s at X + s*ldx (ldx >= nx*ny*nz).
+ * Complex (k-point) states follow the reference's per-state split layout
+ * {re[N], im[N]} (lobpcg_z_multi_mpi.h:1005-1012): state s holds its real part
+ * at X + s*ldx and its imaginary part at X + s*ldx + N, with ldx >= 2N.
+ */
+#ifndef QUMASUN_B200_H
+#define QUMASUN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QG_API_VERSION 1
+
+typedef enum qg_status {
+    QG_OK = 0,
+    QG_ERR_INVALID = -1,       /* bad argument */
+    QG_ERR_CUDA = -2,          /* CUDA runtime error or no device */
+    QG_ERR_NOMEM = -3,         /* device allocation failed */
+    QG_ERR_CHOLESKY = -4,      /* Gram matrix B not positive definite */
+    QG_ERR_TIMEOUT = -5,       /* a bounded device wait gave up */
+    QG_ERR_NONFINITE = -6,     /* NaN/Inf met in inputs or iterates */
+    QG_ERR_UNSUPPORTED = -7,   /* shape or option this build does not handle */
+    QG_ERR_LIBRARY = -8,       /* cuBLAS / cuSOLVER / cuFFT error */
+    QG_ERR_NOT_CONVERGED = -9  /* solver hit its iteration limit (results still written) */
+} qg_status;
+
+typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1 } qg_precision;
+
+typedef struct qg_context_s* qg_context;
+typedef struct qg_hamiltonian_s* qg_hamiltonian;
+
+/*
+ * Hamiltonian description. The projector tables are the reference's own
+ * per-atom cube form (PP_nonlocal_each_atom, PseudoPotOperator.h:21-24), as
+ * tabulated by UpdatePosition (PseudoPotOperator.h:453-466):
+ *  - projector k of atom a lives on the cube cube[6*(a*n_proj+k) + 0..5] =
+ *    {begin_x, begin_y, begin_z, size_x, size_y, size_z} (GridForSphere,
+ *    GridSubgrid.h:482-492; begins may be negative, the grid is periodic),
+ *    values w_data[w_off[a*n_proj+k] + ...] x-fastest;
+ *  - Y_lm of atom a, lm = l*l + (m + l), lives on the cube of the first
+ *    projector with that l, values ylm_data[ylm_off[a*n_lm+lm] + ...].
+ * The operator applied is the reference's mHamiltonianMatrix_ddm
+ * (qumasun_mpi.matrix.h:20-43, kpoint: qumasun_kpoint.matrix.h:25-50):
+ *   H psi = V psi + sum_atoms sum_k E_k sum_m |p_km> dV <p_km|psi> - 1/2 Lap psi
+ * with p_k0 = w_k * Y00 for l = 0 and p_km = w_k * Y_lm for l >= 1
+ * (ProjectionPP, PseudoPotOperator.h:740-772).
+ * g = (gx, gy, gz) is the Bloch vector in bohr^-1 for the k-point operator
+ * -(1/2)(Lap + 2i g.grad - g^2) (GridDifferenceKpoint8th.h:18-122); it is only
+ * used by the complex entry points and must be zero for the real ones.
+ * All pointers are HOST pointers; the library copies what it needs.
+ */
+typedef struct qg_hamiltonian_desc {
+    int nx, ny, nz;
+    double hx, hy, hz;
+    int fd_order;              /* 2, 4 (the reference's composed 7-point stencil), 6, 8 */
+    const double* V;           /* nx*ny*nz local potential (Ha) */
+    int n_atoms;
+    const double* atom_pos;    /* 3*n_atoms (bohr), informational */
+    int n_proj;                /* projectors per atom (0 = no nonlocal term) */
+    const int* proj_l;         /* n_proj angular momenta, 0..3 */
+    const double* proj_E;      /* n_proj energies E_k (Ha) */
+    const int* cube;           /* 6*n_atoms*n_proj */
+    const double* w_data;
+    const long long* w_off;    /* n_atoms*n_proj */
+    int n_lm;                  /* (max l + 1)^2 */
+    const double* ylm_data;
+    const long long* ylm_off;  /* n_atoms*n_lm */
+    double gx, gy, gz;         /* Bloch vector (complex operator only) */
+} qg_hamiltonian_desc;
+
+/* ---- status / context -------------------------------------------------- */
+const char* qg_status_string(int status);
+int qg_version(void);
+
+/* Creates a context on CUDA device `device` with its own non-blocking stream.
+ * Replaces nothing in the reference (the reference has no device state). */
+int qg_context_create(int device, qg_context* out);
+int qg_context_destroy(qg_context ctx);
+/* Work of this context is issued on `stream` (a cudaStream_t) from now on;
+ * NULL restores the context's own stream. */
+int qg_context_set_stream(qg_context ctx, void* stream);
+int qg_context_synchronize(qg_context ctx);
+
+/* ---- Hamiltonian ------------------------------------------------------- */
+/* Builds the device operator: uploads V, compacts the cube tables into
+ * sphere point lists (gather side) and a per-grid-point entry list (scatter
+ * side). Replaces PseudoPotIntegrator::UpdatePosition (PseudoPotOperator.h:453)
+ * plus the state QUMASUN_SINGLE/QUMASUN_MPI hold for mHamiltonianMatrix. */
+int qg_hamiltonian_create(qg_context ctx, const qg_hamiltonian_desc* desc, qg_hamiltonian* out);
+int qg_hamiltonian_destroy(qg_hamiltonian ham);
+/* Changes the Bloch vector of an existing operator (k-point loop). */
+int qg_hamiltonian_set_kvector(qg_hamiltonian ham, double gx, double gy, double gz);
+
+/* HX[s] = H X[s] for ns states, DEVICE pointers, FP64.
+ * Replaces ns calls of OpeA -> mHamiltonianMatrix(_ddm) (qumasun_single.matrix.h:19-40,
+ * qumasun_mpi.matrix.h:20-43) and the bundled mHamiltonianMatrix_bundle_ddm (:46-104). */
+int qg_hamiltonian_apply_d(qg_hamiltonian ham, int ns, const double* X, long long ldx,
+                           double* HX, long long ldhx);
+/* Same in FP32 (float states; V and projector tables rounded from FP64 once). */
+int qg_hamiltonian_apply_f(qg_hamiltonian ham, int ns, const float* X, long long ldx,
+                           float* HX, long long ldhx);
+/* Same as qg_hamiltonian_apply_d with HOST buffers: copies X to the device,
+ * applies H, copies HX back, and returns after HX is on the host. */
+int qg_hamiltonian_apply_host_d(qg_hamiltonian ham, int ns, const double* X, double* HX);
+
+/* qg_hamiltonian_apply_d with device-side phase timing: *ms_project receives
+ * the projector gather-contraction time and *ms_stencil the fused
+ * stencil + V + projector-scatter time (CUDA events on the context stream;
+ * the call synchronizes). Replaces the StopWatch sectors 13 (PPNonlocal) and
+ * 11/12 (K- and V-operation) of qumasun_mpi.matrix.h:29-41. */
+int qg_hamiltonian_apply_timed_d(qg_hamiltonian ham, int ns, const double* X, long long ldx,
+                                 double* HX, long long ldhx, float* ms_project, float* ms_stencil);
+/* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
+int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUMASUN_B200_H */

@@ -1,0 +1,292 @@
+/*
+ * ref_harness.cpp -- C entry points around the reference's own CPU code.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is compiled by oracle/Makefile against
+ * the reference's headers where they lie (QUMASUN source/), into
+ * oracle/_ref/libqumasun_ref.so. Only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline legs of bench.py load it, as the checker and the timed CPU
+ * baseline. Nothing in the product links or calls it.
+ *
+ * Each entry point drives one reference function unchanged:
+ *   ref_laplacian          -> Laplasian{2nd,4th,6th,8th}_halo
+ *                             (GridDifference2nd.h:1052, 4th.h:544, 6th.h:440, 8th.h:153)
+ *   ref_laplacian_kpoint8  -> LaplasianKpoint8th_halo<KX,KY,KZ> (GridDifferenceKpoint8th.h:124),
+ *                             dispatched on |g| < 1e-8 like LaplasianKpoint8th_ddm (:325-368)
+ *   ref_hamiltonian_apply  -> mHamiltonianMatrix_ddm order (qumasun_mpi.matrix.h:20-43):
+ *                             zero, mPotentialMatrix (V*psi), ProjectionPP
+ *                             (PseudoPotOperator.h:740-772), kinetic Laplacian (coef -1/2)
+ *   ref_lobpcg_d_multi     -> EigenLOBPCG_d_multi (lobpcg_d_multi.h:23-545)
+ *   ref_grid_for_sphere    -> GridForSphere (GridSubgrid.h:482-492)
+ *   ref_ylm_cube           -> SetYlmAround<L,M> (PseudoPotOperator.h:58-71)
+ *
+ * The projector tables are injected in the reference's own cube form
+ * (PP_nonlocal_each_atom: one SubspaceField per projector w_k and per Y_lm),
+ * so the reference's ProjectionPP runs on exactly the arrays the GPU receives.
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+#include <map>
+#include <string>
+#include <complex>
+#include <algorithm>
+#include <random>
+#include <locale>
+#include <type_traits>
+#include <unistd.h>
+#include <fcntl.h>
+
+#include "GridRange.h"
+#include "GridDifference2nd.h"
+#include "GridDifference4th.h"
+#include "GridDifference6th.h"
+#include "GridDifference8th.h"
+#include "GridDifferenceKpoint8th.h"
+#include "w_dsygvx.h"
+
+/* lobpcg_d_multi.h:209 and :284 call lapack_DSYGVX with six arguments while
+ * w_dsygvx.h:25 declares five; the fifth (a factor workspace) is unused by
+ * the solve. This adapter must be declared before the template is parsed. */
+inline int lapack_DSYGVX(double* A, double* B, double* ev, double* evec, double* /*factors*/, int N) {
+    return lapack_DSYGVX(A, B, ev, evec, N);
+}
+#include "lobpcg_d_multi.h"
+
+/* PseudoPotIntegrator_single keeps its per-atom tables private; the harness
+ * fills them directly instead of going through the .vps radial loader. */
+#define private public
+#define protected public
+#include "PseudoPotOperator.h"
+#undef private
+#undef protected
+
+namespace {
+
+struct NullWatch {
+    void Record(int) {}
+    void Record(int, int) {}
+};
+
+struct QuietStdout {
+    int saved = -1;
+    explicit QuietStdout(bool on) {
+        if (!on) return;
+        fflush(stdout);
+        saved = dup(1);
+        int devnull = open("/dev/null", O_WRONLY);
+        dup2(devnull, 1);
+        close(devnull);
+    }
+    ~QuietStdout() {
+        if (saved < 0) return;
+        fflush(stdout);
+        dup2(saved, 1);
+        close(saved);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+/* Hamiltonian description passed from Python (flat arrays, FP64). */
+typedef struct ref_ham_desc {
+    int nx, ny, nz;
+    double hx, hy, hz;
+    int fd_order;            /* 2, 4 (the reference's composed 7-point stencil), 6, 8 */
+    const double* V;         /* nx*ny*nz local potential */
+    int n_atoms;
+    const double* atom_pos;  /* 3*n_atoms */
+    int n_proj;              /* projectors per atom */
+    const int* proj_l;       /* n_proj */
+    const double* proj_E;    /* n_proj */
+    const int* cube;         /* n_atoms*n_proj*6: begin xyz, size xyz of projector k's cube */
+    const double* w_data;    /* concatenated w cubes */
+    const long long* w_off;  /* n_atoms*n_proj offsets into w_data */
+    int n_lm;                /* (lmax+1)^2 */
+    const double* ylm_data;  /* concatenated Y_lm cubes (cube of the first projector with that l) */
+    const long long* ylm_off;/* n_atoms*n_lm offsets */
+} ref_ham_desc;
+
+int ref_grid_for_sphere(double Rx, double Ry, double Rz, double rc, double hx, double hy, double hz,
+                        int* out6) {
+    GridRange g = GridForSphere(Rx, Ry, Rz, rc, hx, hy, hz);
+    out6[0] = g.begin_x; out6[1] = g.begin_y; out6[2] = g.begin_z;
+    out6[3] = g.end_x;   out6[4] = g.end_y;   out6[5] = g.end_z;
+    return 0;
+}
+
+int ref_ylm_cube(int l, int m, const int* begin3, const int* size3, const double* R3,
+                 const double* h3, double* out) {
+#define QG_YLM_CASE(L, M)                                                                   \
+    if (l == L && m == M) {                                                                 \
+        SetYlmAround<L, M>(out, begin3[0], begin3[1], begin3[2], size3[0], size3[1], size3[2], \
+                           R3[0], R3[1], R3[2], h3[0], h3[1], h3[2]);                         \
+        return 0;                                                                           \
+    }
+    QG_YLM_CASE(0, 0)
+    QG_YLM_CASE(1, -1) QG_YLM_CASE(1, 0) QG_YLM_CASE(1, 1)
+    QG_YLM_CASE(2, -2) QG_YLM_CASE(2, -1) QG_YLM_CASE(2, 0) QG_YLM_CASE(2, 1) QG_YLM_CASE(2, 2)
+#undef QG_YLM_CASE
+    return -1;
+}
+
+/* out += coef * Laplacian(in), periodic, one state. */
+int ref_laplacian(int order, int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                  const double* in, double* out) {
+    GridRange grid{0, 0, 0, nx, ny, nz};
+    int mw = (order == 2) ? 1 : (order == 8) ? 4 : 3;
+    std::vector<double> buf((size_t)(nx + 2 * mw) * (ny + 2 * mw) * (nz + 2 * mw));
+    switch (order) {
+        case 2: Laplasian2nd_halo(grid, out, in, buf.data(), coef, hx, hy, hz); break;
+        case 4: Laplasian4th_halo(grid, out, in, buf.data(), coef, hx, hy, hz); break;
+        case 6: Laplasian6th_halo(grid, out, in, buf.data(), coef, hx, hy, hz); break;
+        case 8: Laplasian8th_halo(grid, out, in, buf.data(), coef, hx, hy, hz); break;
+        default: return -1;
+    }
+    return 0;
+}
+
+/* out += -(1/2)(nabla^2 + 2 i g.nabla - g^2) psi on split re/im arrays (coef = -1/2). */
+int ref_laplacian_kpoint8(int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                          double gx, double gy, double gz, const double* re, const double* im,
+                          double* out_re, double* out_im) {
+    GridRange grid{0, 0, 0, nx, ny, nz};
+    std::vector<double> bre((size_t)(nx + 8) * (ny + 8) * (nz + 8));
+    std::vector<double> bim(bre.size());
+    SoAComplex out{out_re, out_im};
+    SoAComplex src{const_cast<double*>(re), const_cast<double*>(im)};
+    const double th = 1.0e-8;
+    const int kx = fabs(gx) >= th, ky = fabs(gy) >= th, kz = fabs(gz) >= th;
+    const int sel = kx * 4 + ky * 2 + kz;
+#define QG_KP(A, B, C)                                                                        \
+    case A * 4 + B * 2 + C:                                                                   \
+        LaplasianKpoint8th_halo<A, B, C>(grid, out, src, bre.data(), bim.data(), coef, hx, hy, hz, \
+                                         gx, gy, gz);                                         \
+        break;
+    switch (sel) {
+        QG_KP(0, 0, 0) QG_KP(0, 0, 1) QG_KP(0, 1, 0) QG_KP(0, 1, 1)
+        QG_KP(1, 0, 0) QG_KP(1, 0, 1) QG_KP(1, 1, 0) QG_KP(1, 1, 1)
+    }
+#undef QG_KP
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+/* Owns a PseudoPotIntegrator_single whose tables come from a ref_ham_desc. */
+struct RefHamiltonian {
+    const ref_ham_desc* d;
+    PseudoPotIntegrator_single pp;
+    std::vector<Nucleus> nuclei;
+    std::vector<double> halo;
+
+    explicit RefHamiltonian(const ref_ham_desc* desc) : d(desc) {
+        GridInfo gi;
+        gi.size_x = d->nx; gi.size_y = d->ny; gi.size_z = d->nz;
+        gi.size_3d = (size_t)d->nx * d->ny * d->nz;
+        pp.InitializeGrid(gi, d->hx, d->hy, d->hz);
+        const int Z = 6;
+        if (d->n_atoms > 0 && d->n_proj > 0) {
+            PseudoPot_MBK* mbk = new PseudoPot_MBK();
+            mbk->num_projectors = d->n_proj;
+            mbk->projector_quantum_l = new int[d->n_proj];
+            mbk->projector_energy_up = new double[d->n_proj];
+            for (int k = 0; k < d->n_proj; ++k) {
+                mbk->projector_quantum_l[k] = d->proj_l[k];
+                mbk->projector_energy_up[k] = d->proj_E[k];
+            }
+            pp.m_pp_list.emplace(Z, mbk);
+        }
+        pp.m_pp_by_atom.resize(d->n_atoms);
+        for (int a = 0; a < d->n_atoms; ++a) {
+            nuclei.push_back(Nucleus{Z, d->atom_pos[3 * a], d->atom_pos[3 * a + 1], d->atom_pos[3 * a + 2]});
+            PP_nonlocal_each_atom& at = pp.m_pp_by_atom[a];
+            for (int k = 0; k < d->n_proj; ++k) {
+                const int* c = d->cube + 6 * ((size_t)a * d->n_proj + k);
+                at.projector.emplace_back(c[0], c[1], c[2], c[3], c[4], c[5]);
+                double* buf = at.projector.back().Reserve();
+                std::memcpy(buf, d->w_data + d->w_off[(size_t)a * d->n_proj + k],
+                            sizeof(double) * at.projector.back().num_total_grid);
+            }
+            for (int lm = 0; lm < d->n_lm; ++lm) {
+                int l = (int)std::floor(std::sqrt((double)lm) + 1e-9);
+                int kfirst = -1;
+                for (int k = 0; k < d->n_proj; ++k) if (d->proj_l[k] == l) { kfirst = k; break; }
+                const int* c = d->cube + 6 * ((size_t)a * d->n_proj + (kfirst < 0 ? 0 : kfirst));
+                at.Ylm.emplace_back(c[0], c[1], c[2], c[3], c[4], c[5]);
+                double* buf = at.Ylm.back().Reserve();
+                std::memcpy(buf, d->ylm_data + d->ylm_off[(size_t)a * d->n_lm + lm],
+                            sizeof(double) * at.Ylm.back().num_total_grid);
+            }
+        }
+        int mw = (d->fd_order == 2) ? 1 : (d->fd_order == 8) ? 4 : 3;
+        halo.resize((size_t)(d->nx + 2 * mw) * (d->ny + 2 * mw) * (d->nz + 2 * mw));
+    }
+
+    ~RefHamiltonian() {
+        for (auto& at : pp.m_pp_by_atom) {
+            for (auto& f : at.projector) f.Release();
+            for (auto& f : at.Ylm) f.Release();
+        }
+    }
+
+    /* One state, in the order of mHamiltonianMatrix_ddm (qumasun_mpi.matrix.h:20-43). */
+    void Apply(double* Hp, const double* phi) {
+        const size_t N = (size_t)d->nx * d->ny * d->nz;
+        vecmath::SetZero<double>(Hp, N);
+        for (size_t i = 0; i < N; ++i) Hp[i] = d->V[i] * phi[i];
+        if (d->n_atoms > 0 && d->n_proj > 0) {
+            RspaceFunc<double> hp(Hp);
+            RspaceFunc<double> ps(const_cast<double*>(phi));
+            pp.ProjectionPP(hp, ps, nuclei.data(), (int)nuclei.size());
+        }
+        GridRange grid{0, 0, 0, d->nx, d->ny, d->nz};
+        switch (d->fd_order) {
+            case 2: Laplasian2nd_halo(grid, Hp, phi, halo.data(), -0.5, d->hx, d->hy, d->hz); break;
+            case 4: Laplasian4th_halo(grid, Hp, phi, halo.data(), -0.5, d->hx, d->hy, d->hz); break;
+            case 6: Laplasian6th_halo(grid, Hp, phi, halo.data(), -0.5, d->hx, d->hy, d->hz); break;
+            default: Laplasian8th_halo(grid, Hp, phi, halo.data(), -0.5, d->hx, d->hy, d->hz); break;
+        }
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+/* HX[s] = H X[s] for ns states, state-major (X[s*N + i]). */
+int ref_hamiltonian_apply(const ref_ham_desc* d, int ns, const double* X, double* HX) {
+    if (d->fd_order != 2 && d->fd_order != 4 && d->fd_order != 6 && d->fd_order != 8) return -1;
+    RefHamiltonian H(d);
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    for (int s = 0; s < ns; ++s) H.Apply(HX + (size_t)s * N, X + (size_t)s * N);
+    return 0;
+}
+
+/* The reference's serial block LOBPCG, run unchanged with the reference H as OpeA.
+ * X (ns*N) in/out, P (ns*N) in/out (the "keep" block), ev (ns) out.
+ * *iters receives the number of LOBPCG iterations taken (counted from OpeA calls). */
+int ref_lobpcg_d_multi(const ref_ham_desc* d, int ns, int iter_max, double* ev, double* X,
+                       double* P, int is_first_time, int quiet, int* iters) {
+    RefHamiltonian H(d);
+    const int N = d->nx * d->ny * d->nz;
+    const double dV = d->hx * d->hy * d->hz;
+    std::vector<double> work(WorkSizeLOBPCG_d_multi(N, ns));
+    long long calls = 0;
+    auto OpeA = [&](double* Ax, double* x) { ++calls; H.Apply(Ax, x); };
+    NullWatch watch;
+    {
+        QuietStdout q(quiet != 0);
+        EigenLOBPCG_d_multi(N, dV, ns, iter_max, ev, X, P, work.data(), is_first_time != 0, OpeA, watch);
+    }
+    if (iters) *iters = (int)((calls - 2LL * ns) / ns);
+    return 0;
+}
+
+}  // extern "C"

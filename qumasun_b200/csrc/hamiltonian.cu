@@ -1,0 +1,691 @@
+// Kohn-Sham H|psi> on the device: fused FD stencil + local potential + nonlocal
+// projector scatter (one kernel), after a projector gather-contraction kernel.
+//
+//   k_project   : c[s][a,ch] = E_ch * dV * sum_{p in sphere(a)} tab[ch][p] * psi_s[g(p)]
+//                 (InnerProd_1S_1R / InnerProd_2S_1R of ProjectionPP,
+//                  PseudoPotOperator.h:740-772, all atoms and channels at once)
+//   k_hamiltonian: HX_s = V psi_s + sum_{entries e of g} sum_ch val[e][ch] c[s][a_e,ch]
+//                         + (-1/2) Lap psi_s
+//                 (mHamiltonianMatrix_ddm, qumasun_mpi.matrix.h:20-43; the Add_1S/Add_2S
+//                  scatter of ProjectionPP becomes a per-point gather so no atomics
+//                  are needed; the stencils follow Laplasian{2,4,6,8}th_halo_f).
+//
+// Stencil data flow (per thread block: one state, ty full x-rows, a slab of z):
+// the block marches up z; each thread keeps its own column's 2R+1 z-values in
+// registers, stages the current plane (ty rows + R halo rows above and below,
+// and R wrapped columns left and right) in shared memory for the x/y
+// neighbours, and prefetches the plane R+1 ahead while it computes.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "qg_internal.h"
+
+namespace qg {
+
+int stencil_radius(int order) {
+    switch (order) {
+        case 2: return 1;
+        case 4: return 3;
+        case 6: return 3;
+        case 8: return 4;
+        default: return -1;
+    }
+}
+
+int pick_tile_rows(int nx, int ny) {
+    int best = 0;
+    for (int t = 1; t <= 16; ++t)
+        if (ny % t == 0 && nx * t <= 1024) best = t;
+    return best;
+}
+
+template <typename T>
+struct HamArgs {
+    const T* X;
+    long long ldx;
+    T* HX;
+    long long ldhx;
+    int ns;
+    const T* V;
+    int nx, ny, nz;
+    int ty;
+    int zslab;
+    T c0;
+    T cx[4], cy[4], cz[4];
+    // nonlocal scatter side (row == nullptr: no nonlocal term)
+    const int* row;
+    const int* ent_atom;
+    const T* ent_val;
+    int nch;
+    int ncoef;       // na * nch
+    const T* coef;   // [ns][ncoef]
+};
+
+__device__ __forceinline__ int wrap_idx(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// Laplacian at one point. p points at the centre in the staged plane (row pitch W);
+// q holds the centre's column z-values q[R-R..R+R].
+template <typename T, int ORDER, int R>
+__device__ __forceinline__ T stencil_point(const T* __restrict__ p, int W, const T* q,
+                                           const HamArgs<T>& a) {
+    const T c = q[R];
+    if constexpr (ORDER == 2) {
+        // Laplasian2nd_halo_f (GridDifference2nd.h:1027-1031)
+        return a.cx[0] * (p[1] + p[-1] - T(2) * c) + a.cy[0] * (p[W] + p[-W] - T(2) * c) +
+               a.cz[0] * (q[R + 1] + q[R - 1] - T(2) * c);
+    } else if constexpr (ORDER == 4) {
+        // Laplasian4th_halo_f (GridDifference4th.h:528-530), composed 7-point stencil
+        return a.cx[2] * ((p[3] + p[-3]) - T(54) * (p[2] + p[-2]) + T(783) * (p[1] + p[-1]) - T(1460) * c) +
+               a.cy[2] * ((p[3 * W] + p[-3 * W]) - T(54) * (p[2 * W] + p[-2 * W]) +
+                          T(783) * (p[W] + p[-W]) - T(1460) * c) +
+               a.cz[2] * ((q[R + 3] + q[R - 3]) - T(54) * (q[R + 2] + q[R - 2]) +
+                          T(783) * (q[R + 1] + q[R - 1]) - T(1460) * c);
+    } else if constexpr (ORDER == 6) {
+        // Laplasian6th_halo_f (GridDifference6th.h:425-429)
+        T d = a.c0 * c;
+        d += a.cx[2] * (p[3] + p[-3]) + a.cx[1] * (p[2] + p[-2]) + a.cx[0] * (p[1] + p[-1]);
+        d += a.cy[2] * (p[3 * W] + p[-3 * W]) + a.cy[1] * (p[2 * W] + p[-2 * W]) + a.cy[0] * (p[W] + p[-W]);
+        d += a.cz[2] * (q[R + 3] + q[R - 3]) + a.cz[1] * (q[R + 2] + q[R - 2]) + a.cz[0] * (q[R + 1] + q[R - 1]);
+        return d;
+    } else {
+        // Laplasian8th_halo_f (GridDifference8th.h:141-145)
+        T d = a.c0 * c;
+        d += a.cx[3] * (p[4] + p[-4]) + a.cx[2] * (p[3] + p[-3]) + a.cx[1] * (p[2] + p[-2]) + a.cx[0] * (p[1] + p[-1]);
+        d += a.cy[3] * (p[4 * W] + p[-4 * W]) + a.cy[2] * (p[3 * W] + p[-3 * W]) +
+             a.cy[1] * (p[2 * W] + p[-2 * W]) + a.cy[0] * (p[W] + p[-W]);
+        d += a.cz[3] * (q[R + 4] + q[R - 4]) + a.cz[2] * (q[R + 3] + q[R - 3]) +
+             a.cz[1] * (q[R + 2] + q[R - 2]) + a.cz[0] * (q[R + 1] + q[R - 1]);
+        return d;
+    }
+}
+
+// One thread block: states [s0, s0+SPB), grid rows [y0, y0+ty), planes [zs, ze).
+// blockDim.x == nx*ty (each thread owns one (ix, iy) column).
+template <typename T, int ORDER, int SPB>
+__global__ void __launch_bounds__(1024) k_hamiltonian(const HamArgs<T> a) {
+    constexpr int R = ORDER == 2 ? 1 : (ORDER == 8 ? 4 : 3);
+    constexpr int Q = 2 * R + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
+    const int W = nx + 2 * R;
+    const int rows = ty + 2 * R;
+    const int t = threadIdx.x;
+    const int ix = t % nx;
+    const int ly = t / nx;
+    const int y0 = blockIdx.x * ty;
+    const int iy = y0 + ly;
+    const int s0 = blockIdx.y * SPB;
+    const int zs = blockIdx.z * a.zslab;
+    const int ze = min(nz, zs + a.zslab);
+    if (zs >= ze) return;
+    const long long plane = (long long)nx * ny;
+    const long long col = (long long)iy * nx + ix;
+
+    const T* Xs[SPB];
+    bool valid[SPB];
+#pragma unroll
+    for (int s = 0; s < SPB; ++s) {
+        valid[s] = (s0 + s) < a.ns;
+        Xs[s] = a.X + (long long)(valid[s] ? s0 + s : s0) * a.ldx;
+    }
+
+    T q[SPB][Q];
+#pragma unroll
+    for (int s = 0; s < SPB; ++s)
+#pragma unroll
+        for (int d = 0; d < Q; ++d) q[s][d] = Xs[s][wrap_idx(zs - R + d, nz) * plane + col];
+
+    for (int z = zs; z < ze; ++z) {
+        // prefetch the plane entering the register window next step
+        T nq[SPB];
+        const bool more = (z + 1) < ze;
+        if (more) {
+            const long long off = (long long)wrap_idx(z + R + 1, nz) * plane + col;
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) nq[s] = Xs[s][off];
+        }
+        // stage this plane's interior value (and its wrapped x copies)
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            T* ps = sm + s * rows * W + (R + ly) * W;
+            const T v = q[s][R];
+            ps[R + ix] = v;
+            if (ix < R) ps[R + nx + ix] = v;
+            if (ix >= nx - R) ps[ix - (nx - R)] = v;
+        }
+        // halo rows above and below the tile (wrapped in y)
+        const long long zoff = (long long)z * plane;
+        for (int h = t; h < 2 * R * nx; h += blockDim.x) {
+            const int hr = h / nx, hx = h % nx;
+            const int src = wrap_idx(hr < R ? y0 - R + hr : y0 + ty + (hr - R), ny);
+            const int dst = hr < R ? hr : ty + hr;
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+                const T v = Xs[s][zoff + (long long)src * nx + hx];
+                T* ps = sm + s * rows * W + dst * W;
+                ps[R + hx] = v;
+                if (hx < R) ps[R + nx + hx] = v;
+                if (hx >= nx - R) ps[hx - (nx - R)] = v;
+            }
+        }
+        __syncthreads();
+
+        const long long gi = zoff + col;
+        const T vloc = a.V[gi];
+        T nl[SPB];
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) nl[s] = T(0);
+        if (a.row) {
+            const int e0 = a.row[gi], e1 = a.row[gi + 1];
+            for (int e = e0; e < e1; ++e) {
+                const int at = a.ent_atom[e];
+                const T* ev = a.ent_val + (long long)e * a.nch;
+                for (int ch = 0; ch < a.nch; ++ch) {
+                    const T tv = ev[ch];
+#pragma unroll
+                    for (int s = 0; s < SPB; ++s)
+                        nl[s] += tv * a.coef[(long long)(valid[s] ? s0 + s : s0) * a.ncoef + at * a.nch + ch];
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < SPB; ++s) {
+            const T* pc = sm + s * rows * W + (R + ly) * W + R + ix;
+            const T lap = stencil_point<T, ORDER, R>(pc, W, q[s], a);
+            const T out = (vloc * q[s][R] + nl[s]) + lap;
+            if (valid[s]) a.HX[(long long)(s0 + s) * a.ldhx + gi] = out;
+        }
+        __syncthreads();
+        if (more) {
+#pragma unroll
+            for (int s = 0; s < SPB; ++s) {
+#pragma unroll
+                for (int d = 0; d < Q - 1; ++d) q[s][d] = q[s][d + 1];
+                q[s][Q - 1] = nq[s];
+            }
+        }
+    }
+}
+
+// Gather-contraction of the projectors: one block per (atom, group of SB states).
+template <typename T, int SB, int NCH>
+__global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long long ldx, int ns,
+                                                 const int* __restrict__ atom_off,
+                                                 const int* __restrict__ pt_g,
+                                                 const T* __restrict__ tab, long long npts,
+                                                 const double* __restrict__ ch_scale,
+                                                 T* __restrict__ coef, int ncoef) {
+    const int atom = blockIdx.x;
+    const int s0 = blockIdx.y * SB;
+    const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
+    T acc[SB][NCH];
+#pragma unroll
+    for (int s = 0; s < SB; ++s)
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) acc[s][c] = T(0);
+    const T* Xs[SB];
+#pragma unroll
+    for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
+
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        const int g = pt_g[p];
+        T tv[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) tv[c] = tab[(long long)c * npts + p];
+#pragma unroll
+        for (int s = 0; s < SB; ++s) {
+            const T v = Xs[s][g];
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) acc[s][c] += tv[c] * v;
+        }
+    }
+    // block reduction: warp shuffles, then one value per warp through shared memory
+    __shared__ T red[8][SB * NCH];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < SB; ++s)
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            T v = acc[s][c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][s * NCH + c] = v;
+        }
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < SB * NCH; i += blockDim.x) {
+        T v = T(0);
+        for (int w = 0; w < nw; ++w) v += red[w][i];
+        const int s = i / NCH, c = i % NCH;
+        if (s0 + s < ns)
+            coef[(long long)(s0 + s) * ncoef + atom * NCH + c] = T(ch_scale[atom * NCH + c] * (double)v);
+    }
+}
+
+template <typename T, int NCH>
+static void launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X,
+                               long long ldx, T* coef, cudaStream_t st) {
+    const int blocks_per_sb8 = pj.na * ((ns + 7) / 8);
+    if (blocks_per_sb8 >= 2 * 148) {
+        dim3 g(pj.na, (ns + 7) / 8);
+        k_project<T, 8, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
+                                                pj.ch_scale, coef, pj.na * NCH);
+    } else if (pj.na * ((ns + 1) / 2) >= 2 * 148) {
+        dim3 g(pj.na, (ns + 1) / 2);
+        k_project<T, 2, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
+                                                pj.ch_scale, coef, pj.na * NCH);
+    } else {
+        dim3 g(pj.na, ns);
+        k_project<T, 1, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
+                                                pj.ch_scale, coef, pj.na * NCH);
+    }
+}
+
+template <typename T>
+static int launch_project(const DevProjectors& pj, int ns, const T* X, long long ldx, T* coef,
+                          cudaStream_t st) {
+    const T* tab;
+    if constexpr (sizeof(T) == 8) tab = reinterpret_cast<const T*>(pj.tab_d);
+    else tab = reinterpret_cast<const T*>(pj.tab_f);
+    switch (pj.nch) {
+        case 4: launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, st); break;
+        case 8: launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, st); break;
+        case 16: launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, st); break;
+        default: return QG_ERR_UNSUPPORTED;
+    }
+    return QG_OK;
+}
+
+template <typename T, int ORDER>
+static int launch_stencil(const HamArgs<T>& a, int nz, cudaStream_t st) {
+    constexpr int R = ORDER == 2 ? 1 : (ORDER == 8 ? 4 : 3);
+    constexpr int SPB = 1;
+    const int tiles = a.ny / a.ty;
+    const int sgroups = (a.ns + SPB - 1) / SPB;
+    // enough blocks for every SM: split z into slabs when the (tile, state) grid is small
+    long long base = (long long)tiles * sgroups;
+    int nslab = 1;
+    const long long target = 4LL * 148;
+    if (base < target) nslab = (int)std::min<long long>((target + base - 1) / base, std::max(1, nz / (2 * R)));
+    HamArgs<T> b = a;
+    b.zslab = (nz + nslab - 1) / nslab;
+    nslab = (nz + b.zslab - 1) / b.zslab;
+    const size_t smem = (size_t)SPB * (a.ty + 2 * R) * (a.nx + 2 * R) * sizeof(T);
+    auto kern = k_hamiltonian<T, ORDER, SPB>;
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return QG_ERR_UNSUPPORTED;
+    }
+    dim3 grid(tiles, sgroups, nslab);
+    kern<<<grid, a.nx * a.ty, smem, st>>>(b);
+    return QG_OK;
+}
+
+template <typename T>
+int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
+                      T* coef, cudaStream_t st, cudaEvent_t ev_mid) {
+    const DevProjectors& pj = h->pj;
+    HamArgs<T> a{};
+    a.X = X; a.ldx = ldx; a.HX = HX; a.ldhx = ldhx; a.ns = ns;
+    if constexpr (sizeof(T) == 8) a.V = reinterpret_cast<const T*>(h->V_d);
+    else a.V = reinterpret_cast<const T*>(h->V_f);
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.ty = h->ty;
+    // coefficients of -1/2 Lap exactly as the reference forms them
+    const double coefk = -0.5;
+    const double ih[3] = {h->hx, h->hy, h->hz};
+    T* cs[3] = {a.cx, a.cy, a.cz};
+    switch (h->order) {
+        case 2:
+            a.c0 = T(-coefk * (2.0 / (ih[0] * ih[0]) + 2.0 / (ih[1] * ih[1]) + 2.0 / (ih[2] * ih[2])));
+            for (int d = 0; d < 3; ++d) cs[d][0] = T(coefk / (ih[d] * ih[d]));
+            break;
+        case 4:
+            for (int d = 0; d < 3; ++d) {
+                const double s = (24.0 * ih[d]) * (24.0 * ih[d]);
+                cs[d][2] = T(coefk / s);
+                cs[d][1] = T(-54.0 * coefk / s);
+                cs[d][0] = T(783.0 * coefk / s);
+            }
+            break;
+        case 6:
+            a.c0 = T(-245.0 * coefk * (1.0 / (90.0 * ih[0] * ih[0]) + 1.0 / (90.0 * ih[1] * ih[1]) + 1.0 / (90.0 * ih[2] * ih[2])));
+            for (int d = 0; d < 3; ++d) {
+                const double s = 90.0 * ih[d] * ih[d];
+                cs[d][2] = T(coefk / s);
+                cs[d][1] = T(-13.5 * coefk / s);
+                cs[d][0] = T(135.0 * coefk / s);
+            }
+            break;
+        case 8:
+            a.c0 = T(-14350.0 / 5040.0 * coefk * (1.0 / (ih[0] * ih[0]) + 1.0 / (ih[1] * ih[1]) + 1.0 / (ih[2] * ih[2])));
+            for (int d = 0; d < 3; ++d) {
+                const double s = 5040.0 * ih[d] * ih[d];
+                cs[d][3] = T(-9.0 * coefk / s);
+                cs[d][2] = T(128.0 * coefk / s);
+                cs[d][1] = T(-1008.0 * coefk / s);
+                cs[d][0] = T(8064.0 * coefk / s);
+            }
+            break;
+        default: return QG_ERR_INVALID;
+    }
+    if (pj.na > 0 && pj.nch > 0) {
+        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, st));
+        a.row = pj.row;
+        a.ent_atom = pj.ent_atom;
+        if constexpr (sizeof(T) == 8) a.ent_val = reinterpret_cast<const T*>(pj.ent_val_d);
+        else a.ent_val = reinterpret_cast<const T*>(pj.ent_val_f);
+        a.nch = pj.nch;
+        a.ncoef = pj.na * pj.nch;
+        a.coef = coef;
+    }
+    if (ev_mid) QG_CUDA_TRY(cudaEventRecord(ev_mid, st));
+    int rc;
+    switch (h->order) {
+        case 2: rc = launch_stencil<T, 2>(a, h->nz, st); break;
+        case 4: rc = launch_stencil<T, 4>(a, h->nz, st); break;
+        case 6: rc = launch_stencil<T, 6>(a, h->nz, st); break;
+        default: rc = launch_stencil<T, 8>(a, h->nz, st); break;
+    }
+    if (rc != QG_OK) return rc;
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
+
+template int apply_hamiltonian<double>(qg_hamiltonian, int, const double*, long long, double*,
+                                       long long, double*, cudaStream_t, cudaEvent_t);
+template int apply_hamiltonian<float>(qg_hamiltonian, int, const float*, long long, float*,
+                                      long long, float*, cudaStream_t, cudaEvent_t);
+
+}  // namespace qg
+
+// --------------------------------------------------------------------------
+// Host-side table building (once per geometry).
+
+namespace {
+
+int wrap_host(int i, int n) {
+    int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src) {
+    *dst = nullptr;
+    if (src.empty()) return QG_OK;
+    QG_CUDA_TRY(cudaMalloc(dst, src.size() * sizeof(T)));
+    QG_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return QG_OK;
+}
+
+void free_projectors(DevProjectors& pj) {
+    cudaFree(pj.atom_off); cudaFree(pj.pt_g); cudaFree(pj.tab_d); cudaFree(pj.tab_f);
+    cudaFree(pj.ch_scale); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
+    cudaFree(pj.ent_val_f);
+    pj = DevProjectors{};
+}
+
+// Compacts the reference's per-atom cube tables into sphere point lists and the
+// per-grid-point entry list (see DevProjectors). A cube point is kept when any
+// channel value is nonzero; points outside every cutoff hold exact zeros in the
+// reference tables and add nothing.
+int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
+    const int na = d->n_atoms, np = d->n_proj;
+    if (na <= 0 || np <= 0) return QG_OK;
+    int nch_real = 0;
+    for (int k = 0; k < np; ++k) {
+        if (d->proj_l[k] < 0 || d->proj_l[k] > 3) return QG_ERR_INVALID;
+        nch_real += 2 * d->proj_l[k] + 1;
+    }
+    int nch = nch_real <= 4 ? 4 : (nch_real <= 8 ? 8 : (nch_real <= 16 ? 16 : -1));
+    if (nch < 0) return QG_ERR_UNSUPPORTED;
+    const double Y00 = 1.0 / sqrt(4.0 * M_PI);
+    const double dV = h->hx * h->hy * h->hz;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const long long N = h->N();
+
+    std::vector<int> atom_off(na + 1, 0);
+    std::vector<int> pt_g;
+    std::vector<std::vector<double>> tabs(nch);
+    std::vector<double> ch_scale((size_t)na * nch, 0.0);
+    std::vector<int> ch_k(nch, -1), ch_m(nch, 0);
+    {
+        int c = 0;
+        for (int k = 0; k < np; ++k)
+            for (int m = 0; m < 2 * d->proj_l[k] + 1; ++m) { ch_k[c] = k; ch_m[c] = m; ++c; }
+    }
+    for (int a = 0; a < na; ++a) {
+        int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+        for (int k = 0; k < np; ++k) {
+            const int* c = d->cube + 6 * ((size_t)a * np + k);
+            for (int i = 0; i < 3; ++i) {
+                if (c[3 + i] <= 0) return QG_ERR_INVALID;
+                lo[i] = std::min(lo[i], c[i]);
+                hi[i] = std::max(hi[i], c[i] + c[3 + i]);
+            }
+        }
+        for (int ch = 0; ch < nch; ++ch)
+            ch_scale[(size_t)a * nch + ch] = ch_k[ch] >= 0 ? d->proj_E[ch_k[ch]] * dV : 0.0;
+        std::vector<double> vals(nch);
+        for (int z = lo[2]; z < hi[2]; ++z)
+            for (int y = lo[1]; y < hi[1]; ++y)
+                for (int x = lo[0]; x < hi[0]; ++x) {
+                    bool any = false;
+                    for (int ch = 0; ch < nch; ++ch) {
+                        vals[ch] = 0.0;
+                        const int k = ch_k[ch];
+                        if (k < 0) continue;
+                        const int* c = d->cube + 6 * ((size_t)a * np + k);
+                        const int qx = x - c[0], qy = y - c[1], qz = z - c[2];
+                        if (qx < 0 || qy < 0 || qz < 0 || qx >= c[3] || qy >= c[4] || qz >= c[5]) continue;
+                        const size_t q = qx + (size_t)c[3] * (qy + (size_t)c[4] * qz);
+                        const double w = d->w_data[d->w_off[(size_t)a * np + k] + q];
+                        const int l = d->proj_l[k];
+                        if (l == 0) {
+                            vals[ch] = w * Y00;
+                        } else {
+                            const int lm = l * l + ch_m[ch];
+                            if (lm >= d->n_lm) return QG_ERR_INVALID;
+                            vals[ch] = w * d->ylm_data[d->ylm_off[(size_t)a * d->n_lm + lm] + q];
+                        }
+                        if (vals[ch] != 0.0) any = true;
+                    }
+                    if (!any) continue;
+                    const long long g = wrap_host(x, nx) + (long long)nx * (wrap_host(y, ny) + (long long)ny * wrap_host(z, nz));
+                    pt_g.push_back((int)g);
+                    for (int ch = 0; ch < nch; ++ch) tabs[ch].push_back(vals[ch]);
+                }
+        atom_off[a + 1] = (int)pt_g.size();
+    }
+    const long long npts = (long long)pt_g.size();
+    std::vector<double> tab_d((size_t)nch * npts);
+    for (int ch = 0; ch < nch; ++ch) std::copy(tabs[ch].begin(), tabs[ch].end(), tab_d.begin() + (size_t)ch * npts);
+    std::vector<float> tab_f(tab_d.begin(), tab_d.end());
+
+    // scatter side: per grid point, the (atom, values) entries covering it, atom-ordered
+    std::vector<int> row(N + 1, 0);
+    for (long long p = 0; p < npts; ++p) row[pt_g[p] + 1]++;
+    for (long long g = 0; g < N; ++g) row[g + 1] += row[g];
+    std::vector<int> fill(row.begin(), row.end() - 1);
+    std::vector<int> ent_atom(npts);
+    std::vector<double> ent_val((size_t)npts * nch);
+    for (int a = 0; a < na; ++a)
+        for (int p = atom_off[a]; p < atom_off[a + 1]; ++p) {
+            const int e = fill[pt_g[p]]++;
+            ent_atom[e] = a;
+            for (int ch = 0; ch < nch; ++ch) ent_val[(size_t)e * nch + ch] = tab_d[(size_t)ch * npts + p];
+        }
+    std::vector<float> ent_val_f(ent_val.begin(), ent_val.end());
+
+    DevProjectors& pj = h->pj;
+    pj.na = na; pj.nch = nch; pj.npts = npts; pj.nent = npts;
+    QG_TRY(upload(&pj.atom_off, atom_off));
+    QG_TRY(upload(&pj.pt_g, pt_g));
+    QG_TRY(upload(&pj.tab_d, tab_d));
+    QG_TRY(upload(&pj.tab_f, tab_f));
+    QG_TRY(upload(&pj.ch_scale, ch_scale));
+    QG_TRY(upload(&pj.row, row));
+    QG_TRY(upload(&pj.ent_atom, ent_atom));
+    QG_TRY(upload(&pj.ent_val_d, ent_val));
+    QG_TRY(upload(&pj.ent_val_f, ent_val_f));
+    return QG_OK;
+}
+
+void destroy_ham(qg_hamiltonian h) {
+    if (!h) return;
+    cudaFree(h->V_d);
+    cudaFree(h->V_f);
+    free_projectors(h->pj);
+    h->coef.release();
+    h->xio.release();
+    h->hxio.release();
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qg_hamiltonian_create(qg_context ctx, const qg_hamiltonian_desc* d, qg_hamiltonian* out) {
+    if (!ctx || !d || !out) return QG_ERR_INVALID;
+    *out = nullptr;
+    if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || !(d->hx > 0) || !(d->hy > 0) || !(d->hz > 0) || !d->V)
+        return QG_ERR_INVALID;
+    const int R = qg::stencil_radius(d->fd_order);
+    if (R < 0) return QG_ERR_INVALID;
+    if (d->nx < 2 * R || d->ny < 2 * R || d->nz < 2 * R) return QG_ERR_UNSUPPORTED;
+    if ((long long)d->nx * d->ny * d->nz >= (1LL << 31)) return QG_ERR_UNSUPPORTED;
+    const int ty = qg::pick_tile_rows(d->nx, d->ny);
+    if (ty <= 0) return QG_ERR_UNSUPPORTED;
+    if (d->n_atoms > 0 && d->n_proj > 0 &&
+        (!d->proj_l || !d->proj_E || !d->cube || !d->w_data || !d->w_off || !d->ylm_off))
+        return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(ctx->device));
+    qg_hamiltonian h = new qg_hamiltonian_s();
+    h->ctx = ctx;
+    h->nx = d->nx; h->ny = d->ny; h->nz = d->nz;
+    h->hx = d->hx; h->hy = d->hy; h->hz = d->hz;
+    h->order = d->fd_order;
+    h->gx = d->gx; h->gy = d->gy; h->gz = d->gz;
+    h->ty = ty;
+    const long long N = h->N();
+    std::vector<double> V(d->V, d->V + N);
+    std::vector<float> Vf(V.begin(), V.end());
+    int rc = upload(&h->V_d, V);
+    if (rc == QG_OK) rc = upload(&h->V_f, Vf);
+    if (rc == QG_OK) rc = build_projectors(h, d);
+    if (rc != QG_OK) {
+        destroy_ham(h);
+        return rc;
+    }
+    *out = h;
+    return QG_OK;
+}
+
+int qg_hamiltonian_destroy(qg_hamiltonian h) {
+    if (!h) return QG_ERR_INVALID;
+    cudaSetDevice(h->ctx->device);
+    cudaStreamSynchronize(h->ctx->stream);
+    destroy_ham(h);
+    return QG_OK;
+}
+
+int qg_hamiltonian_set_kvector(qg_hamiltonian h, double gx, double gy, double gz) {
+    if (!h) return QG_ERR_INVALID;
+    h->gx = gx; h->gy = gy; h->gz = gz;
+    return QG_OK;
+}
+
+}  // extern "C"
+
+template <typename T>
+static int apply_device(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx) {
+    if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
+    if (ns == 0) return QG_OK;
+    const long long N = h->N();
+    if (ldx < N || ldhx < N) return QG_ERR_INVALID;
+    if (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    T* coef = nullptr;
+    if (h->pj.na > 0) {
+        QG_TRY(h->coef.reserve((size_t)ns * h->pj.na * h->pj.nch * sizeof(T)));
+        coef = h->coef.as<T>();
+    }
+    return qg::apply_hamiltonian<T>(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream);
+}
+
+extern "C" {
+
+int qg_hamiltonian_apply_d(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX,
+                           long long ldhx) {
+    return apply_device<double>(h, ns, X, ldx, HX, ldhx);
+}
+
+int qg_hamiltonian_apply_f(qg_hamiltonian h, int ns, const float* X, long long ldx, float* HX,
+                           long long ldhx) {
+    return apply_device<float>(h, ns, X, ldx, HX, ldhx);
+}
+
+int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long long ldx,
+                                 double* HX, long long ldhx, float* ms_project, float* ms_stencil) {
+    if (!h || ns <= 0 || !X || !HX) return QG_ERR_INVALID;
+    const long long N = h->N();
+    if (ldx < N || ldhx < N) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    double* coef = nullptr;
+    if (h->pj.na > 0) {
+        QG_TRY(h->coef.reserve((size_t)ns * h->pj.na * h->pj.nch * sizeof(double)));
+        coef = h->coef.as<double>();
+    }
+    cudaEvent_t e0, e1, e2;
+    QG_CUDA_TRY(cudaEventCreate(&e0));
+    QG_CUDA_TRY(cudaEventCreate(&e1));
+    QG_CUDA_TRY(cudaEventCreate(&e2));
+    cudaStream_t st = h->ctx->stream;
+    int rc = QG_OK;
+    if (cudaEventRecord(e0, st) != cudaSuccess) rc = QG_ERR_CUDA;
+    if (rc == QG_OK) rc = qg::apply_hamiltonian<double>(h, ns, X, ldx, HX, ldhx, coef, st, e1);
+    if (rc == QG_OK && cudaEventRecord(e2, st) != cudaSuccess) rc = QG_ERR_CUDA;
+    if (rc == QG_OK && cudaEventSynchronize(e2) != cudaSuccess) rc = QG_ERR_CUDA;
+    float a = 0.f, b = 0.f;
+    if (rc == QG_OK) {
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, e1, e2);
+    }
+    if (ms_project) *ms_project = a;
+    if (ms_stencil) *ms_stencil = b;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    return rc;
+}
+
+int qg_hamiltonian_launches_per_apply(qg_hamiltonian h, int ns) {
+    if (!h || ns < 0) return QG_ERR_INVALID;
+    if (ns == 0) return 0;
+    return (h->pj.na > 0 ? 1 : 0) + 1;
+}
+
+int qg_hamiltonian_apply_host_d(qg_hamiltonian h, int ns, const double* X, double* HX) {
+    if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
+    if (ns == 0) return QG_OK;
+    const long long N = h->N();
+    const size_t bytes = (size_t)ns * N * sizeof(double);
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    QG_TRY(h->xio.reserve(bytes));
+    QG_TRY(h->hxio.reserve(bytes));
+    cudaStream_t st = h->ctx->stream;
+    QG_CUDA_TRY(cudaMemcpyAsync(h->xio.ptr, X, bytes, cudaMemcpyHostToDevice, st));
+    QG_TRY(apply_device<double>(h, ns, h->xio.as<double>(), N, h->hxio.as<double>(), N));
+    QG_CUDA_TRY(cudaMemcpyAsync(HX, h->hxio.ptr, bytes, cudaMemcpyDeviceToHost, st));
+    QG_CUDA_TRY(cudaStreamSynchronize(st));
+    return QG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,102 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "../../include/qumasun_b200.h"
+
+#define QG_CUDA_TRY(expr)                                                       \
+    do {                                                                        \
+        cudaError_t qg_e_ = (expr);                                             \
+        if (qg_e_ != cudaSuccess) {                                             \
+            qg_set_last_error(#expr, cudaGetErrorString(qg_e_), __FILE__, __LINE__); \
+            return qg_e_ == cudaErrorMemoryAllocation ? QG_ERR_NOMEM : QG_ERR_CUDA; \
+        }                                                                       \
+    } while (0)
+
+#define QG_TRY(expr)                    \
+    do {                                \
+        int qg_s_ = (expr);             \
+        if (qg_s_ != QG_OK) return qg_s_; \
+    } while (0)
+
+void qg_set_last_error(const char* what, const char* msg, const char* file, int line);
+
+struct qg_context_s {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    void* blas = nullptr;      // cublasHandle_t, created on first use
+    void* solver = nullptr;    // cusolverDnHandle_t, created on first use
+};
+
+// A device buffer that only grows.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t want) {
+        if (want <= bytes) return QG_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&ptr, want) != cudaSuccess) return QG_ERR_NOMEM;
+        bytes = want;
+        return QG_OK;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Nonlocal projector tables on the device, in two orders:
+//  gather side (atom-major): atom a owns points [atom_off[a], atom_off[a+1]) of
+//    pt_g (grid index) and tab[ch*npts + p] (channel values w*Y);
+//  scatter side (grid-point-major): grid point g owns entries
+//    [row[g], row[g+1]) with the atom id ent_atom[e] and channel values
+//    ent_val[e*nch + ch].
+struct DevProjectors {
+    int na = 0, nch = 0;
+    long long npts = 0, nent = 0;
+    int* atom_off = nullptr;
+    int* pt_g = nullptr;
+    double* tab_d = nullptr;
+    float* tab_f = nullptr;
+    double* ch_scale = nullptr;  // E_k * dV per (atom, channel)
+    int* row = nullptr;
+    int* ent_atom = nullptr;
+    double* ent_val_d = nullptr;
+    float* ent_val_f = nullptr;
+};
+
+struct qg_hamiltonian_s {
+    qg_context ctx = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    double hx = 0, hy = 0, hz = 0;
+    int order = 8;
+    double gx = 0, gy = 0, gz = 0;
+    double* V_d = nullptr;
+    float* V_f = nullptr;
+    DevProjectors pj;
+    DevBuf coef;      // projector coefficients E*dV*<p|psi>, [ns][na*nch]
+    DevBuf xio, hxio; // staging for the host-buffer entry point
+    int ty = 1;       // grid rows per stencil tile
+    long long N() const { return (long long)nx * ny * nz; }
+};
+
+namespace qg {
+
+// Stencil tile geometry: ty grid rows of full x-rows per thread block.
+int pick_tile_rows(int nx, int ny);
+int stencil_radius(int order);
+
+// Launchers (hamiltonian.cu).
+template <typename T>
+int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
+                      T* coef_scratch, cudaStream_t st, cudaEvent_t ev_mid = nullptr);
+
+}  // namespace qg

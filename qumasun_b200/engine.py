@@ -1,0 +1,218 @@
+"""ctypes binding of the engine's C ABI (include/qumasun_b200.h).
+
+Mirrors the reference's operator interface for the H|psi> path: a Hamiltonian
+is built once per geometry from the reference's cube tables
+(PseudoPotIntegrator::UpdatePosition, PseudoPotOperator.h:453-466) and then
+applied to blocks of states (the OpeA callback of qumasun_single.lobpcg.h:19-23,
+batched). There is no CPU path: if the shared library or a CUDA device is
+missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqumasun_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_longlong)
+
+QG_OK = 0
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device out of memory",
+    -4: "Gram matrix not positive definite", -5: "bounded device wait timed out",
+    -6: "non-finite value", -7: "unsupported shape or option", -8: "CUDA library error",
+    -9: "not converged within the iteration limit",
+}
+
+
+class QGError(RuntimeError):
+    def __init__(self, status, where, detail=""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({status}) {detail}".strip())
+
+
+class HamiltonianDesc(C.Structure):
+    """qg_hamiltonian_desc."""
+
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double),
+        ("fd_order", C.c_int),
+        ("V", _dp),
+        ("n_atoms", C.c_int),
+        ("atom_pos", _dp),
+        ("n_proj", C.c_int),
+        ("proj_l", _ip),
+        ("proj_E", _dp),
+        ("cube", _ip),
+        ("w_data", _dp),
+        ("w_off", _lp),
+        ("n_lm", C.c_int),
+        ("ylm_data", _dp),
+        ("ylm_off", _lp),
+        ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded engine library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python -m qumasun_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.qg_status_string.restype = C.c_char_p
+        L.qg_last_error.restype = C.c_char_p
+        L.qg_context_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.qg_context_destroy.argtypes = [vp]
+        L.qg_context_set_stream.argtypes = [vp, vp]
+        L.qg_context_synchronize.argtypes = [vp]
+        L.qg_hamiltonian_create.argtypes = [vp, C.POINTER(HamiltonianDesc), C.POINTER(vp)]
+        L.qg_hamiltonian_destroy.argtypes = [vp]
+        L.qg_hamiltonian_set_kvector.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+        L.qg_hamiltonian_apply_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
+        L.qg_hamiltonian_apply_f.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
+        L.qg_hamiltonian_apply_host_d.argtypes = [vp, C.c_int, vp, vp]
+        L.qg_hamiltonian_apply_timed_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong,
+                                                   C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
+        _lib = L
+    return _lib
+
+
+def check(status, where):
+    if status != QG_OK:
+        detail = lib().qg_last_error().decode(errors="replace")
+        raise QGError(status, where, detail)
+
+
+class Context:
+    """A device context (qg_context): one CUDA device, one stream."""
+
+    def __init__(self, device=0):
+        self.h = C.c_void_p()
+        check(lib().qg_context_create(device, C.byref(self.h)), "qg_context_create")
+        self.device = device
+
+    def set_stream(self, stream_ptr):
+        check(lib().qg_context_set_stream(self.h, C.c_void_p(stream_ptr)), "qg_context_set_stream")
+
+    def synchronize(self):
+        check(lib().qg_context_synchronize(self.h), "qg_context_synchronize")
+
+    def close(self):
+        if self.h:
+            lib().qg_context_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+class Hamiltonian:
+    """The device operator H = V + V_NL - 1/2 Lap (qg_hamiltonian).
+
+    ``cell`` is a :class:`qumasun_b200.cell.Cell` (or any object with the same
+    fields and ``desc_arrays()``).
+    """
+
+    def __init__(self, ctx: Context, cell, fd_order=None, kvec=(0.0, 0.0, 0.0)):
+        self.ctx = ctx
+        self.cell = cell
+        self.N = cell.N
+        self._arrays = a = cell.desc_arrays()
+        d = HamiltonianDesc()
+        d.nx, d.ny, d.nz = cell.nx, cell.ny, cell.nz
+        d.hx, d.hy, d.hz = cell.hx, cell.hy, cell.hz
+        d.fd_order = int(fd_order if fd_order is not None else cell.fd_order)
+        d.V = _ptr(a["V"], _dp)
+        npj = len(cell.proj_l)
+        d.n_atoms = cell.n_atoms if npj else 0
+        d.atom_pos = _ptr(a["atom_pos"], _dp)
+        d.n_proj = npj
+        d.proj_l = _ptr(a["proj_l"], _ip) if npj else None
+        d.proj_E = _ptr(a["proj_E"], _dp) if npj else None
+        d.cube = _ptr(a["cube"], _ip)
+        d.w_data = _ptr(a["w_data"], _dp)
+        d.w_off = _ptr(a["w_off"], _lp)
+        d.n_lm = cell.n_lm
+        d.ylm_data = _ptr(a["ylm_data"], _dp)
+        d.ylm_off = _ptr(a["ylm_off"], _lp)
+        d.gx, d.gy, d.gz = kvec
+        self.desc = d
+        self.h = C.c_void_p()
+        check(lib().qg_hamiltonian_create(ctx.h, C.byref(d), C.byref(self.h)), "qg_hamiltonian_create")
+
+    def apply_device(self, ns, x_ptr, hx_ptr, ldx=None, ldhx=None, dtype="f64"):
+        """HX = H X on device pointers (int addresses), state-major."""
+        ldx = self.N if ldx is None else ldx
+        ldhx = self.N if ldhx is None else ldhx
+        fn = lib().qg_hamiltonian_apply_d if dtype == "f64" else lib().qg_hamiltonian_apply_f
+        check(fn(self.h, ns, C.c_void_p(x_ptr), ldx, C.c_void_p(hx_ptr), ldhx),
+              "qg_hamiltonian_apply_" + ("d" if dtype == "f64" else "f"))
+
+    def apply(self, X, out=None):
+        """HX = H X for torch CUDA tensors (ns, N) of float64 or float32."""
+        import torch
+        assert X.is_cuda and X.dim() == 2 and X.shape[1] == self.N
+        X = X.contiguous()
+        if out is None:
+            out = torch.empty_like(X)
+        dt = "f64" if X.dtype == torch.float64 else "f32"
+        if dt == "f32" and X.dtype != torch.float32:
+            raise TypeError("states must be float64 or float32")
+        self.apply_device(X.shape[0], X.data_ptr(), out.data_ptr(), dtype=dt)
+        return out
+
+    def apply_timed(self, ns, x_ptr, hx_ptr):
+        """FP64 apply with device phase times: returns (ms_project, ms_stencil)."""
+        a, b = C.c_float(), C.c_float()
+        check(lib().qg_hamiltonian_apply_timed_d(self.h, ns, C.c_void_p(x_ptr), self.N,
+                                                 C.c_void_p(hx_ptr), self.N, C.byref(a), C.byref(b)),
+              "qg_hamiltonian_apply_timed_d")
+        return a.value, b.value
+
+    def launches_per_apply(self, ns):
+        return lib().qg_hamiltonian_launches_per_apply(self.h, ns)
+
+    def apply_host(self, X: np.ndarray, out: np.ndarray | None = None):
+        """HX = H X with host buffers (copies in and out inside the call)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        if out is None:
+            out = np.empty_like(X)
+        check(lib().qg_hamiltonian_apply_host_d(self.h, X.shape[0], X.ctypes.data, out.ctypes.data),
+              "qg_hamiltonian_apply_host_d")
+        return out
+
+    def apply_host_ptr(self, ns, x_ptr, hx_ptr):
+        check(lib().qg_hamiltonian_apply_host_d(self.h, ns, C.c_void_p(x_ptr), C.c_void_p(hx_ptr)),
+              "qg_hamiltonian_apply_host_d")
+
+    def close(self):
+        if self.h:
+            lib().qg_hamiltonian_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

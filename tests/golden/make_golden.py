@@ -1,0 +1,84 @@
+"""Generates tests/golden/*.npz from the reference's own code (oracle/_ref).
+
+Run where the reference tree exists and `make -C oracle` has built
+oracle/_ref/libqumasun_ref.so:  python tests/golden/make_golden.py
+Every array comes from the reference functions driven by oracle/ref_harness.cpp:
+Laplasian{2,4,6,8}th_halo, LaplasianKpoint8th_halo, the reference Hamiltonian
+(V, ProjectionPP, kinetic) and GridForSphere / SetYlmAround tables.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from qumasun_b200.cell import build_cell, initial_states  # noqa: E402
+
+# small cells: (name, build_cell kwargs). "wrap" has projector cubes larger than
+# the cell, so a grid point is covered by several periodic images of one atom.
+CASES = [
+    ("noncubic", dict(grid=(20, 16, 24))),
+    ("wrap", dict(grid=(12, 12, 12), a0=4.4)),
+]
+
+
+def main():
+    for name, kw in CASES:
+        cell = build_cell(**kw)
+        X = initial_states(2, cell.N, seed=7)
+        out = dict(X=X, grid=np.array([cell.nx, cell.ny, cell.nz]),
+                   h=np.array([cell.hx, cell.hy, cell.hz]), V=cell.V,
+                   positions=cell.positions)
+        for order in (2, 4, 6, 8):
+            out[f"HX{order}"] = O.hamiltonian_apply(cell, X, impl="ref", fd_order=order)
+            out[f"LAP{order}"] = O.laplacian(order, (cell.nx, cell.ny, cell.nz),
+                                             (cell.hx, cell.hy, cell.hz), -0.5, X[0], impl="ref")
+        g = (0.31, -0.17, 0.05)
+        ore, oim = O.laplacian_kpoint8((cell.nx, cell.ny, cell.nz), (cell.hx, cell.hy, cell.hz),
+                                       -0.5, g, X[0], X[1], impl="ref")
+        out["kp_g"] = np.array(g)
+        out["KP_re"], out["KP_im"] = ore, oim
+        # the reference's own projector-cube geometry and Y_lm tables for atom 0
+        lib = O.ref_lib()
+        import ctypes as C
+        R = cell.positions[0]
+        c6 = (C.c_int * 6)()
+        lib.ref_grid_for_sphere(R[0], R[1], R[2], cell.cutoff, cell.hx, cell.hy, cell.hz, c6)
+        b = np.array(c6[:3], dtype=np.int32)
+        s = np.array([c6[3] - c6[0], c6[4] - c6[1], c6[5] - c6[2]], dtype=np.int32)
+        out["cube0"] = np.concatenate([b, s])
+        for lm, (l, m) in enumerate([(0, 0), (1, -1), (1, 0), (1, 1)]):
+            buf = np.zeros(int(np.prod(s)))
+            Rv = np.ascontiguousarray(R, dtype=np.float64)
+            hv = np.array([cell.hx, cell.hy, cell.hz])
+            lib.ref_ylm_cube(l, m, b.ctypes.data_as(C.POINTER(C.c_int)), s.ctypes.data_as(C.POINTER(C.c_int)),
+                             Rv.ctypes.data_as(C.POINTER(C.c_double)), hv.ctypes.data_as(C.POINTER(C.c_double)),
+                             buf.ctypes.data_as(C.POINTER(C.c_double)))
+            out[f"Y{lm}"] = buf
+        np.savez_compressed(os.path.join(HERE, f"ham_{name}.npz"), **out)
+        print("wrote", name)
+    # the reference's serial block LOBPCG (EigenLOBPCG_d_multi) on a small cell
+    cell = build_cell(grid=(16, 16, 16))
+    X0 = initial_states(6, cell.N, seed=11)
+    r = O.ref_lobpcg_d_multi(cell, X0, 2000)
+    np.savez_compressed(os.path.join(HERE, "lobpcg_small.npz"), grid=np.array([16, 16, 16]),
+                        ns=6, seed=11, ev=r["ev"], iters=r["iters"])
+    print("wrote lobpcg_small", r["iters"], r["ev"])
+
+
+if __name__ == "__main__":
+    main()
+
+# lobpcg_diamond8.npz (the 8-atom 40^3 cell, 16 states, seed 1234, FD order 8) is
+# the output of oracle.ref_lobpcg_d_multi(build_cell(), initial_states(16, 64000,
+# seed=1234), 3000): 435 iterations, about 3 minutes on one core. Regenerate with
+#   python tests/golden/make_golden.py --diamond8
+if __name__ == "__main__" and "--diamond8" in sys.argv:
+    cell = build_cell()
+    r = O.ref_lobpcg_d_multi(cell, initial_states(16, cell.N, seed=1234), 3000)
+    np.savez_compressed(os.path.join(HERE, "lobpcg_diamond8.npz"), ev=r["ev"], iters=r["iters"], ns=16,
+                        seed=1234, seconds=r["seconds"])

@@ -1,0 +1,142 @@
+"""H|psi> on the B200 against the CPU oracle (port pinned to the reference)
+and the reference's golden fixtures. Tolerances: FP64 1e-12 relative per state
+(norm-wise), FP32 2e-6 relative per state against the FP64 oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from qumasun_b200.cell import build_cell, initial_states
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL64 = 1e-12
+TOL32 = 2e-6
+
+
+def rel_per_state(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+
+
+def gpu_apply(ctx, cell, X, order=None, dtype="f64"):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    H = Hamiltonian(ctx, cell, fd_order=order)
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).to("cuda", tdt)
+    out = H.apply(Xd)
+    torch.cuda.synchronize()
+    H.close()
+    return out.double().cpu().numpy()
+
+
+@pytest.mark.parametrize("name,kw", [("noncubic", dict(grid=(20, 16, 24))),
+                                     ("wrap", dict(grid=(12, 12, 12), a0=4.4))])
+@pytest.mark.parametrize("order", [2, 4, 6, 8])
+def test_fp64_matches_reference_golden(cuda_ctx, name, kw, order):
+    g = np.load(os.path.join(GOLD, f"ham_{name}.npz"))
+    cell = build_cell(**kw)
+    HX = gpu_apply(cuda_ctx, cell, g["X"], order)
+    assert rel_per_state(HX, g[f"HX{order}"]).max() < TOL64
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 8])
+def test_fp64_and_fp32_match_oracle_diamond8(cuda_ctx, order):
+    cell = build_cell()  # 8 atoms, 40^3
+    X = initial_states(16, cell.N, seed=21)
+    ref = O.hamiltonian_apply(cell, X, fd_order=order)
+    assert rel_per_state(gpu_apply(cuda_ctx, cell, X, order), ref).max() < TOL64
+    assert rel_per_state(gpu_apply(cuda_ctx, cell, X.astype(np.float32), order, "f32"), ref).max() < TOL32
+
+
+def test_displaced_cell_no_nonlocal_and_no_potential(cuda_ctx):
+    for kw in [dict(grid=(24, 20, 16), displacement=0.3, seed=5),
+               dict(grid=(16, 16, 16), nonlocal_on=False),
+               dict(grid=(16, 24, 16), potential_on=False)]:
+        cell = build_cell(**kw)
+        X = initial_states(5, cell.N, seed=8)
+        ref = O.hamiltonian_apply(cell, X)
+        assert rel_per_state(gpu_apply(cuda_ctx, cell, X), ref).max() < TOL64
+
+
+def test_strided_states_and_empty_batch(cuda_ctx):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(grid=(16, 16, 16))
+    N = cell.N
+    X = initial_states(3, N, seed=4)
+    ld = N + 40
+    Xp = torch.zeros(3, ld, dtype=torch.float64, device="cuda")
+    Xp[:, :N] = torch.from_numpy(X).cuda()
+    HXp = torch.full((3, ld), 7.0, dtype=torch.float64, device="cuda")
+    H = Hamiltonian(cuda_ctx, cell)
+    H.apply_device(3, Xp.data_ptr(), HXp.data_ptr(), ldx=ld, ldhx=ld)
+    H.apply_device(0, Xp.data_ptr(), HXp.data_ptr())  # no-op
+    torch.cuda.synchronize()
+    out = HXp.cpu().numpy()
+    assert np.all(out[:, N:] == 7.0)  # padding untouched
+    assert rel_per_state(out[:, :N], O.hamiltonian_apply(cell, X)).max() < TOL64
+    H.close()
+
+
+def test_host_entry_point_matches_device(cuda_ctx):
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(grid=(20, 20, 20))
+    X = initial_states(4, cell.N, seed=6)
+    H = Hamiltonian(cuda_ctx, cell)
+    HXh = H.apply_host(X)
+    H.close()
+    np.testing.assert_array_equal(HXh, gpu_apply(cuda_ctx, cell, X))
+    assert rel_per_state(HXh, O.hamiltonian_apply(cell, X)).max() < TOL64
+
+
+def test_invalid_arguments_are_rejected(cuda_ctx):
+    from qumasun_b200 import Hamiltonian, QGError
+    cell = build_cell(grid=(16, 16, 16))
+    with pytest.raises(QGError):
+        Hamiltonian(cuda_ctx, cell, fd_order=5)
+    H = Hamiltonian(cuda_ctx, cell)
+    with pytest.raises(QGError):
+        H.apply_device(2, 0, 0)
+    with pytest.raises(QGError):
+        H.apply_device(1, 16, 16, ldx=10)
+    H.close()
+
+
+def test_diamond64_full_batch_properties(cuda_ctx):
+    """64 atoms, 80^3, 256 states: sampled states against the oracle, and the
+    size-independent properties of the whole batch (symmetry of H, linearity)."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(reps=(2, 2, 2))
+    ns = 256
+    H = Hamiltonian(cuda_ctx, cell)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.rand(ns, cell.N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    HX = H.apply(X)
+    torch.cuda.synchronize()
+    pick = [0, 77, 255]
+    ref = O.hamiltonian_apply(cell, X[pick].cpu().numpy())
+    assert rel_per_state(HX[pick].cpu().numpy(), ref).max() < TOL64
+    G = (X @ HX.T) * cell.dV            # <x_i|H|x_j>
+    asym = (G - G.T).abs().max().item() / G.abs().max().item()
+    assert asym < 1e-12
+    a, b = 0.3, -1.7
+    Y = torch.roll(X, 1, 0)
+    lin = H.apply(a * X + b * Y) - (a * HX + b * H.apply(Y))
+    assert (lin.norm(dim=1) / HX.norm(dim=1)).max().item() < 1e-12
+    Xf = X.float()
+    HXf = H.apply(Xf)
+    torch.cuda.synchronize()
+    assert ((HXf.double() - HX).norm(dim=1) / HX.norm(dim=1)).max().item() < TOL32
+    H.close()
+
+
+def test_diamond216_sampled_states(cuda_ctx):
+    """216 atoms, 120^3, displaced: a few states against the oracle."""
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(reps=(3, 3, 3), displacement=0.05, seed=0)
+    X = initial_states(3, cell.N, seed=31)
+    ref = O.hamiltonian_apply(cell, X)
+    assert rel_per_state(gpu_apply(cuda_ctx, cell, X), ref).max() < TOL64

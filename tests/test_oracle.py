@@ -1,0 +1,82 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures made by
+tests/golden/make_golden.py from oracle/_ref, i.e. the reference headers)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from qumasun_b200.cell import build_cell, grid_for_sphere, initial_states
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+CASES = {"noncubic": dict(grid=(20, 16, 24)), "wrap": dict(grid=(12, 12, 12), a0=4.4)}
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    name = request.param
+    g = np.load(os.path.join(GOLD, f"ham_{name}.npz"))
+    return name, build_cell(**CASES[name]), g
+
+
+def test_cell_builder_reproduces_fixture_inputs(case):
+    _, cell, g = case
+    assert tuple(g["grid"]) == (cell.nx, cell.ny, cell.nz)
+    np.testing.assert_array_equal(g["V"], cell.V)
+    np.testing.assert_array_equal(g["positions"], cell.positions)
+    np.testing.assert_array_equal(g["X"], initial_states(2, cell.N, seed=7))
+
+
+def test_projector_tables_match_reference_tabulation(case):
+    # GridForSphere (GridSubgrid.h:482-492) and SetYlmAround<L,M> (PseudoPotOperator.h:58-71)
+    _, cell, g = case
+    R = cell.positions[0]
+    b, e = grid_for_sphere(R, cell.cutoff, (cell.hx, cell.hy, cell.hz))
+    np.testing.assert_array_equal(g["cube0"], np.array(b + [e[i] - b[i] for i in range(3)]))
+    for lm in range(4):
+        np.testing.assert_allclose(cell.ylm_tabs[0][lm], g[f"Y{lm}"], rtol=0, atol=2e-16)
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 8])
+def test_port_laplacian_matches_reference(case, order):
+    _, cell, g = case
+    lap = O.laplacian(order, (cell.nx, cell.ny, cell.nz), (cell.hx, cell.hy, cell.hz), -0.5, g["X"][0])
+    assert rel(lap, g[f"LAP{order}"]) < 1e-15
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 8])
+def test_port_hamiltonian_matches_reference(case, order):
+    _, cell, g = case
+    HX = O.hamiltonian_apply(cell, g["X"], impl="port", fd_order=order)
+    for s in range(2):
+        assert rel(HX[s], g[f"HX{order}"][s]) < 1e-14
+
+
+def test_port_kpoint_laplacian_matches_reference(case):
+    _, cell, g = case
+    ore, oim = O.laplacian_kpoint8((cell.nx, cell.ny, cell.nz), (cell.hx, cell.hy, cell.hz), -0.5,
+                                   tuple(g["kp_g"]), g["X"][0], g["X"][1])
+    np.testing.assert_array_equal(ore, g["KP_re"])
+    np.testing.assert_array_equal(oim, g["KP_im"])
+
+
+def test_port_lobpcg_matches_reference_eigenvalues_and_iterations():
+    g = np.load(os.path.join(GOLD, "lobpcg_small.npz"))
+    cell = build_cell(grid=tuple(g["grid"]))
+    X0 = initial_states(int(g["ns"]), cell.N, seed=int(g["seed"]))
+    r = O.lobpcg_d_multi(lambda X: O.hamiltonian_apply(cell, X), X0, cell.dV, 2000)
+    assert r["iters"] == int(g["iters"])
+    np.testing.assert_allclose(r["ev"], g["ev"], rtol=0, atol=1e-10)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_port_matches_live_reference_on_fresh_cell():
+    cell = build_cell(grid=(16, 20, 12), displacement=0.2, seed=3)
+    X = initial_states(3, cell.N, seed=99)
+    a = O.hamiltonian_apply(cell, X, impl="port")
+    b = O.hamiltonian_apply(cell, X, impl="ref")
+    assert max(rel(a[s], b[s]) for s in range(3)) < 1e-14
