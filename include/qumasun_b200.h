@@ -88,11 +88,17 @@ int qg_version(void);
 /* Creates a context on CUDA device `device` with its own non-blocking stream.
  * Replaces nothing in the reference (the reference has no device state). */
 int qg_context_create(int device, qg_context* out);
+/* Fails with QG_ERR_INVALID while operators built on the context are alive. */
 int qg_context_destroy(qg_context ctx);
 /* Work of this context is issued on `stream` (a cudaStream_t) from now on;
- * NULL restores the context's own stream. */
+ * NULL selects the CUDA legacy default stream. A new context starts on its
+ * own non-blocking stream. */
 int qg_context_set_stream(qg_context ctx, void* stream);
+/* Waits for the context's stream, then returns (and clears) the device status
+ * word: QG_OK, or QG_ERR_TIMEOUT if a kernel's bounded wait gave up. */
 int qg_context_synchronize(qg_context ctx);
+/* Returns and clears the device status word without waiting for the stream. */
+int qg_context_take_device_status(qg_context ctx);
 
 /* ---- Hamiltonian ------------------------------------------------------- */
 /* Builds the device operator: uploads V, compacts the cube tables into
@@ -116,13 +122,18 @@ int qg_hamiltonian_apply_f(qg_hamiltonian ham, int ns, const float* X, long long
  * applies H, copies HX back, and returns after HX is on the host. */
 int qg_hamiltonian_apply_host_d(qg_hamiltonian ham, int ns, const double* X, double* HX);
 
-/* qg_hamiltonian_apply_d with device-side phase timing: *ms_project receives
- * the projector gather-contraction time and *ms_stencil the fused
- * stencil + V + projector-scatter time (CUDA events on the context stream;
- * the call synchronizes). Replaces the StopWatch sectors 13 (PPNonlocal) and
- * 11/12 (K- and V-operation) of qumasun_mpi.matrix.h:29-41. */
+/* qg_hamiltonian_apply_d with device-side phase timing (CUDA events on the
+ * context stream; the call synchronizes): ms_phases[0] = projector
+ * gather-contraction, [1] = stencil + local potential, [2] = nonlocal scatter
+ * (the fused kernel reports its scatter inside [1]). Replaces the StopWatch
+ * sectors 13 (PPNonlocal), 11 (K-operation) and 12 (V-operation) of
+ * qumasun_mpi.matrix.h:29-41. */
 int qg_hamiltonian_apply_timed_d(qg_hamiltonian ham, int ns, const double* X, long long ldx,
-                                 double* HX, long long ldhx, float* ms_project, float* ms_stencil);
+                                 double* HX, long long ldhx, float* ms_phases);
+/* Selects the stencil kernel of an operator: 0 = the TMA-staged ring kernel
+ * where the shape and alignment allow (default), 1 = always the
+ * register-window kernel (any shape). Both compute the same operator. */
+int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int plain);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
 

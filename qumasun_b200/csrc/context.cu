@@ -51,6 +51,12 @@ int qg_context_create(int device, qg_context* out) {
         return QG_ERR_CUDA;
     }
     c->stream = c->own_stream;
+    if (cudaMalloc(&c->dev_status, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->dev_status, 0, sizeof(int)) != cudaSuccess) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return QG_ERR_CUDA;
+    }
     *out = c;
     return QG_OK;
 }
@@ -64,19 +70,21 @@ void qg_release_libraries(qg_context c) {
 
 int qg_context_destroy(qg_context c) {
     if (!c) return QG_ERR_INVALID;
+    if (c->live_hamiltonians > 0) return QG_ERR_INVALID;
     cudaSetDevice(c->device);
     qg_release_libraries(c);
     if (c->own_stream) {
         cudaStreamSynchronize(c->own_stream);
         cudaStreamDestroy(c->own_stream);
     }
+    if (c->dev_status) cudaFree(c->dev_status);
     delete c;
     return QG_OK;
 }
 
 int qg_context_set_stream(qg_context c, void* stream) {
     if (!c) return QG_ERR_INVALID;
-    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    c->stream = static_cast<cudaStream_t>(stream);
     return QG_OK;
 }
 
@@ -84,7 +92,16 @@ int qg_context_synchronize(qg_context c) {
     if (!c) return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(c->device));
     QG_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return QG_OK;
+    return qg_context_take_device_status(c);
 }
+
+int qg_context_take_device_status(qg_context c) {
+    if (!c) return QG_ERR_INVALID;
+    int v = 0;
+    QG_CUDA_TRY(cudaMemcpy(&v, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v != 0) QG_CUDA_TRY(cudaMemset(c->dev_status, 0, sizeof(int)));
+    return v;
+}
+
 
 }  // extern "C"

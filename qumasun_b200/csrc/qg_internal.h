@@ -30,6 +30,8 @@ struct qg_context_s {
     cudaStream_t stream = nullptr;
     void* blas = nullptr;      // cublasHandle_t, created on first use
     void* solver = nullptr;    // cusolverDnHandle_t, created on first use
+    int live_hamiltonians = 0; // the context outlives every operator built on it
+    int* dev_status = nullptr; // device status word set by kernels whose bounded waits gave up
 };
 
 // A device buffer that only grows.
@@ -85,6 +87,19 @@ struct qg_hamiltonian_s {
     DevBuf coef;      // projector coefficients E*dV*<p|psi>, [ns][na*nch]
     DevBuf xio, hxio; // staging for the host-buffer entry point
     int ty = 1;       // grid rows per stencil tile
+    int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
+    int use_graph = 1;            // replay the chunked pipeline from a captured CUDA graph
+    cudaStream_t side[2] = {nullptr, nullptr};  // projection and scatter streams of the pipeline
+    std::vector<cudaEvent_t> evs;               // pipeline events (timing disabled)
+    struct GraphCache {
+        cudaGraphExec_t exec = nullptr;
+        int ns = 0, dtype = 0;
+        const void* X = nullptr;
+        void* HX = nullptr;
+        long long ldx = 0, ldhx = 0;
+        cudaStream_t st = nullptr;
+        const void* coef = nullptr;
+    } graph;
     long long N() const { return (long long)nx * ny * nz; }
 };
 
@@ -95,8 +110,39 @@ int pick_tile_rows(int nx, int ny);
 int stencil_radius(int order);
 
 // Launchers (hamiltonian.cu).
+// Device-time accounting by phase: mark(tag) records an event; the time up to
+// the next mark is charged to `tag` (0 projection, 1 stencil + V, 2 scatter).
+struct PhaseTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> tag;
+    void mark(int t, cudaStream_t st) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        ev.push_back(e);
+        tag.push_back(t);
+    }
+    void totals(float* ms3) {
+        ms3[0] = ms3[1] = ms3[2] = 0.f;
+        if (!ev.empty()) cudaEventSynchronize(ev.back());
+        for (size_t i = 0; i + 1 < ev.size(); ++i) {
+            float d = 0.f;
+            cudaEventElapsedTime(&d, ev[i], ev[i + 1]);
+            if (tag[i] >= 0 && tag[i] < 3) ms3[tag[i]] += d;
+        }
+    }
+    ~PhaseTimer() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+int chunk_states(long long N, size_t elem);
+int project_splits(const DevProjectors& pj);
+// Elements of projector-coefficient scratch one apply of ns states needs.
+size_t coef_scratch_elems(qg_hamiltonian h, int ns, size_t elem);
+
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
-                      T* coef_scratch, cudaStream_t st, cudaEvent_t ev_mid = nullptr);
+                      T* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
 
 }  // namespace qg

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -85,8 +86,10 @@ def lib():
         L.qg_hamiltonian_apply_f.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_hamiltonian_apply_host_d.argtypes = [vp, C.c_int, vp, vp]
         L.qg_hamiltonian_apply_timed_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong,
-                                                   C.POINTER(C.c_float), C.POINTER(C.c_float)]
+                                                   C.POINTER(C.c_float)]
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
+        L.qg_hamiltonian_set_stencil_kernel.argtypes = [vp, C.c_int]
+        L.qg_context_take_device_status.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -104,6 +107,7 @@ class Context:
         self.h = C.c_void_p()
         check(lib().qg_context_create(device, C.byref(self.h)), "qg_context_create")
         self.device = device
+        self.children = weakref.WeakSet()
 
     def set_stream(self, stream_ptr):
         check(lib().qg_context_set_stream(self.h, C.c_void_p(stream_ptr)), "qg_context_set_stream")
@@ -111,8 +115,19 @@ class Context:
     def synchronize(self):
         check(lib().qg_context_synchronize(self.h), "qg_context_synchronize")
 
+    def take_device_status(self):
+        return lib().qg_context_take_device_status(self.h)
+
+    def use_torch_stream(self):
+        """Issue the engine's work on torch's current CUDA stream (orders it
+        with the surrounding torch operations)."""
+        import torch
+        self.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+
     def close(self):
         if self.h:
+            for child in list(self.children):
+                child.close()
             lib().qg_context_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -160,6 +175,7 @@ class Hamiltonian:
         self.desc = d
         self.h = C.c_void_p()
         check(lib().qg_hamiltonian_create(ctx.h, C.byref(d), C.byref(self.h)), "qg_hamiltonian_create")
+        ctx.children.add(self)
 
     def apply_device(self, ns, x_ptr, hx_ptr, ldx=None, ldhx=None, dtype="f64"):
         """HX = H X on device pointers (int addresses), state-major."""
@@ -179,16 +195,21 @@ class Hamiltonian:
         dt = "f64" if X.dtype == torch.float64 else "f32"
         if dt == "f32" and X.dtype != torch.float32:
             raise TypeError("states must be float64 or float32")
+        self.ctx.use_torch_stream()
         self.apply_device(X.shape[0], X.data_ptr(), out.data_ptr(), dtype=dt)
         return out
 
     def apply_timed(self, ns, x_ptr, hx_ptr):
-        """FP64 apply with device phase times: returns (ms_project, ms_stencil)."""
-        a, b = C.c_float(), C.c_float()
+        """FP64 apply with device phase times (ms): (projection, stencil + V, scatter)."""
+        ph = (C.c_float * 3)()
         check(lib().qg_hamiltonian_apply_timed_d(self.h, ns, C.c_void_p(x_ptr), self.N,
-                                                 C.c_void_p(hx_ptr), self.N, C.byref(a), C.byref(b)),
+                                                 C.c_void_p(hx_ptr), self.N, ph),
               "qg_hamiltonian_apply_timed_d")
-        return a.value, b.value
+        return tuple(ph)
+
+    def set_stencil_kernel(self, plain: bool):
+        """False: TMA-staged ring kernel where the shape allows (default); True: register-window kernel."""
+        check(lib().qg_hamiltonian_set_stencil_kernel(self.h, 1 if plain else 0), "qg_hamiltonian_set_stencil_kernel")
 
     def launches_per_apply(self, ns):
         return lib().qg_hamiltonian_launches_per_apply(self.h, ns)

@@ -20,5 +20,6 @@ def cuda_ctx():
         pytest.fail("gpu test selected but no CUDA device is visible")
     torch.cuda.init()
     ctx = Context(0)
+    ctx.use_torch_stream()
     yield ctx
     ctx.close()
