@@ -1,16 +1,17 @@
-// Kohn-Sham H|psi> on the device: fused FD stencil + local potential + nonlocal
-// projector scatter (one kernel), after a projector gather-contraction kernel.
+// Kohn-Sham H|psi> on the device (mHamiltonianMatrix_ddm, qumasun_mpi.matrix.h:20-43):
+//   H psi = V psi + sum_atoms sum_k E_k sum_m |p_km> dV <p_km|psi> - 1/2 Lap psi.
 //
-//   k_project   : c[s][a,ch] = E_ch * dV * sum_{p in sphere(a)} tab[ch][p] * psi_s[g(p)]
-//                 (InnerProd_1S_1R / InnerProd_2S_1R of ProjectionPP,
-//                  PseudoPotOperator.h:740-772, all atoms and channels at once)
-//   k_hamiltonian: HX_s = V psi_s + sum_{entries e of g} sum_ch val[e][ch] c[s][a_e,ch]
-//                         + (-1/2) Lap psi_s
-//                 (mHamiltonianMatrix_ddm, qumasun_mpi.matrix.h:20-43; the Add_1S/Add_2S
-//                  scatter of ProjectionPP becomes a per-point gather so no atomics
-//                  are needed; the stencils follow Laplasian{2,4,6,8}th_halo_f).
+// Main path (shapes the TMA kernel accepts), three launches for a block of states:
+//   k_project     c[s][a,ch] = E_ch dV sum_{p in sphere(a)} tab[ch][p] psi_s[g(p)]
+//                 (InnerProd_1S_1R / InnerProd_2S_1R of ProjectionPP, PseudoPotOperator.h:740-772,
+//                 all atoms, channels and states at once);
+//   k_stencil_tma H psi = V psi - 1/2 Lap psi (stencil_tma.cu: persistent, TMA-staged);
+//   k_scatter_all H psi[s][g] += sum_{entries e of g} sum_ch val[e][ch] c[s][a_e,ch]
+//                 (Add_1S / Add_2S of ProjectionPP turned into a per-point gather, no atomics).
+// Fallback path (any shape): k_project, then k_hamiltonian, a register-window
+// stencil kernel with the per-point scatter fused in.
 //
-// Stencil data flow (per thread block: one state, ty full x-rows, a slab of z):
+// k_hamiltonian data flow (per thread block: SPB states, ty full x-rows, a slab of z):
 // the block marches up z; each thread keeps its own column's 2R+1 z-values in
 // registers, stages the current plane (ty rows + R halo rows above and below,
 // and R wrapped columns left and right) in shared memory for the x/y
@@ -208,6 +209,7 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
 #pragma unroll
     for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
 
+#pragma unroll 2
     for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const int g = pt_g[p];
         T tv[NCH];
@@ -277,159 +279,40 @@ static int launch_project(const DevProjectors& pj, int ns, const T* X, long long
     return QG_OK;
 }
 
-// Projection for one chunk of cn <= SB states, each atom's points split over
-// gridDim.y blocks whose partial sums are added atomically into coef (zeroed first).
-template <typename T, int SB, int NCH>
-__global__ void __launch_bounds__(256) k_project_chunk(const T* __restrict__ X, long long ldx, int cn,
-                                                       const int* __restrict__ atom_off,
-                                                       const int* __restrict__ pt_g,
-                                                       const T* __restrict__ tab, long long npts,
-                                                       const double* __restrict__ ch_scale,
-                                                       T* __restrict__ coef, int ncoef) {
-    const int atom = blockIdx.x;
-    const int a0 = atom_off[atom], a1 = atom_off[atom + 1];
-    const int per = (a1 - a0 + gridDim.y - 1) / gridDim.y;
-    const int p0 = a0 + blockIdx.y * per;
-    const int p1 = min(a1, p0 + per);
-    T acc[SB][NCH];
-#pragma unroll
-    for (int s = 0; s < SB; ++s)
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) acc[s][c] = T(0);
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-        const int g = pt_g[p];
-        T tv[NCH];
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) tv[c] = tab[(long long)c * npts + p];
-#pragma unroll
-        for (int s = 0; s < SB; ++s) {
-            if (s < cn) {
-                const T v = X[(long long)s * ldx + g];
-#pragma unroll
-                for (int c = 0; c < NCH; ++c) acc[s][c] += tv[c] * v;
-            }
-        }
-    }
-    __shared__ T red[8][SB * NCH];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int s = 0; s < SB; ++s)
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) {
-            T v = acc[s][c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) red[warp][s * NCH + c] = v;
-        }
-    __syncthreads();
-    const int nw = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < SB * NCH; i += blockDim.x) {
-        const int s = i / NCH, c = i % NCH;
-        if (s >= cn) continue;
-        T v = T(0);
-        for (int w = 0; w < nw; ++w) v += red[w][i];
-        coef[((long long)blockIdx.y * cn + s) * ncoef + atom * NCH + c] = T(ch_scale[atom * NCH + c] * (double)v);
-    }
-}
-
-// Nonlocal scatter for one chunk of cn <= C states, one thread per grid point:
-// HX[s][g] += sum over the point's entries e and channels ch of val[e][ch] * coef[s][atom_e, ch].
-// Each table entry is read once for all the chunk's states; HX of the chunk was
-// just written by the stencil kernel and is still in L2.
-// Sums the per-split partial coefficients of one chunk in a fixed order (deterministic).
-template <typename T>
-__global__ void k_coef_reduce(const T* __restrict__ part, T* __restrict__ coef, int n, int nsplit) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T v = T(0);
-    for (int y = 0; y < nsplit; ++y) v += part[(long long)y * n + i];
-    coef[i] = v;
-}
-
-template <typename T, int C, int NCH>
-__global__ void __launch_bounds__(256) k_scatter(T* __restrict__ HX, long long ldhx, int cn, long long N,
-                                                 const int* __restrict__ row,
-                                                 const int* __restrict__ ent_atom,
-                                                 const T* __restrict__ ent_val,
-                                                 const T* __restrict__ coef, int ncoef) {
-    extern __shared__ __align__(16) unsigned char smem_sc[];
-    T* cs = reinterpret_cast<T*>(smem_sc);
-    for (int i = threadIdx.x; i < cn * ncoef; i += blockDim.x) cs[i] = coef[i];
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = g < N;
-    int e0 = 0, e1 = 0;
-    T h[C];
-    if (in) {
-        e0 = row[g];
-        e1 = row[g + 1];
-#pragma unroll
-        for (int s = 0; s < C; ++s) h[s] = (s < cn) ? HX[(long long)s * ldhx + g] : T(0);
-    }
-    __syncthreads();
-    if (!in || e0 == e1) return;
-    T acc[C];
-#pragma unroll
-    for (int s = 0; s < C; ++s) acc[s] = T(0);
-    for (int e = e0; e < e1; ++e) {
-        const int base = ent_atom[e] * NCH;
-        T v[NCH];
-#pragma unroll
-        for (int c = 0; c < NCH; ++c) v[c] = ent_val[(long long)e * NCH + c];
-#pragma unroll
-        for (int s = 0; s < C; ++s) {
-            if (s < cn) {
-#pragma unroll
-                for (int c = 0; c < NCH; ++c) acc[s] += v[c] * cs[s * ncoef + base + c];
-            }
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < C; ++s)
-        if (s < cn) HX[(long long)s * ldhx + g] = h[s] + acc[s];
-}
-
-// Nonlocal scatter over all states, one thread per grid point: the block walks
-// the states in groups of SG, stages the group's coefficients in shared memory,
-// and every thread adds sum_{entries e of g} sum_ch val[e][ch] * coef[s][atom_e, ch]
-// to HX[s][g] for the group (the point's entries are re-read from L1 per group).
+// Nonlocal scatter over all states, one thread per grid point: for each group
+// of SG states it adds sum_{entries e of g} sum_ch val[e][ch] * coef[s][atom_e, ch]
+// to HX[s][g]. The point's entries and the few atoms' coefficients a block
+// touches stay in L1 across the groups.
 template <typename T, int SG, int NCH>
 __global__ void __launch_bounds__(256) k_scatter_all(T* __restrict__ HX, long long ldhx, int ns, long long N,
                                                      const int* __restrict__ row,
                                                      const int* __restrict__ ent_atom,
                                                      const T* __restrict__ ent_val,
                                                      const T* __restrict__ coef, int ncoef) {
-    extern __shared__ __align__(16) unsigned char smem_sa[];
-    T* cs = reinterpret_cast<T*>(smem_sa);
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = g < N;
-    int e0 = 0, e1 = 0;
-    if (in) {
-        e0 = row[g];
-        e1 = row[g + 1];
-    }
-    const bool any = __syncthreads_or(in && e1 > e0);
-    if (!any) return;
+    if (g >= N) return;
+    const int e0 = row[g], e1 = row[g + 1];
+    if (e0 == e1) return;
     for (int s0 = 0; s0 < ns; s0 += SG) {
         const int gn = min(SG, ns - s0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < gn * ncoef; i += blockDim.x) cs[i] = coef[(long long)s0 * ncoef + i];
-        __syncthreads();
-        if (!in || e0 == e1) continue;
         T h[SG];
 #pragma unroll
         for (int s = 0; s < SG; ++s) h[s] = (s < gn) ? HX[(long long)(s0 + s) * ldhx + g] : T(0);
         T acc[SG];
 #pragma unroll
         for (int s = 0; s < SG; ++s) acc[s] = T(0);
+        const T* cg = coef + (long long)s0 * ncoef;
         for (int e = e0; e < e1; ++e) {
-            const int base = ent_atom[e] * NCH;
+            const int base = __ldg(&ent_atom[e]) * NCH;
             T v[NCH];
 #pragma unroll
-            for (int c = 0; c < NCH; ++c) v[c] = ent_val[(long long)e * NCH + c];
+            for (int c = 0; c < NCH; ++c) v[c] = __ldg(&ent_val[(long long)e * NCH + c]);
 #pragma unroll
             for (int s = 0; s < SG; ++s) {
+                if (s < gn) {
 #pragma unroll
-                for (int c = 0; c < NCH; ++c) acc[s] += v[c] * cs[s * ncoef + base + c];
+                    for (int c = 0; c < NCH; ++c) acc[s] += v[c] * __ldg(&cg[s * ncoef + base + c]);
+                }
             }
         }
 #pragma unroll
@@ -445,13 +328,8 @@ static int launch_scatter_all_nch(const DevProjectors& pj, T* HX, long long ldhx
     const T* ev;
     if constexpr (sizeof(T) == 8) ev = reinterpret_cast<const T*>(pj.ent_val_d);
     else ev = reinterpret_cast<const T*>(pj.ent_val_f);
-    const size_t smem = (size_t)SG * pj.na * NCH * sizeof(T);
-    auto kern = k_scatter_all<T, SG, NCH>;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return QG_ERR_UNSUPPORTED;
-    kern<<<(unsigned)((N + 255) / 256), 256, smem, st>>>(HX, ldhx, ns, N, pj.row, pj.ent_atom, ev, coef,
-                                                         pj.na * NCH);
+    k_scatter_all<T, SG, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(HX, ldhx, ns, N, pj.row, pj.ent_atom,
+                                                                           ev, coef, pj.na * NCH);
     return QG_OK;
 }
 
@@ -491,173 +369,10 @@ static int launch_stencil(const HamArgs<T>& a, int nz, cudaStream_t st) {
     return QG_OK;
 }
 
-// States per L2-resident chunk: the chunk's states and results (2 * C * N * sizeof(T))
-// stay within about 80 MB of the 126 MB L2, next to the projector tables.
-int chunk_states(long long N, size_t elem) {
-    const double budget = 20.0e6;
-    for (int c : {16, 8, 4, 2})
-        if ((double)c * (double)N * (double)elem <= budget) return c;
-    return 1;
-}
-
-// Blocks per atom in the chunked projection (each writes its own partial sums).
-int project_splits(const DevProjectors& pj) {
-    const long long avg = pj.npts / std::max(1, pj.na);
-    return (int)std::max<long long>(1, std::min<long long>((4 * 148 + pj.na - 1) / pj.na, avg / 512));
-}
-
-size_t coef_scratch_elems(qg_hamiltonian h, int ns, size_t elem) {
+size_t coef_scratch_elems(qg_hamiltonian h, int ns) {
     const DevProjectors& pj = h->pj;
     if (pj.na <= 0 || pj.nch <= 0) return 0;
-    const size_t ncoef = (size_t)pj.na * pj.nch;
-    // chunked path: per-split partials of one chunk, then the reduced coefficients of every chunk
-    const size_t chunked = (size_t)project_splits(pj) * chunk_states(h->N(), elem) * ncoef + (size_t)ns * ncoef;
-    return std::max((size_t)ns * ncoef, chunked);
-}
-
-template <typename T, int SB, int NCH>
-static void launch_project_chunk_sb(const DevProjectors& pj, int cn, const T* X, long long ldx, T* coef,
-                                    cudaStream_t st) {
-    const T* tab;
-    if constexpr (sizeof(T) == 8) tab = reinterpret_cast<const T*>(pj.tab_d);
-    else tab = reinterpret_cast<const T*>(pj.tab_f);
-    dim3 g(pj.na, project_splits(pj));
-    k_project_chunk<T, SB, NCH><<<g, 256, 0, st>>>(X, ldx, cn, pj.atom_off, pj.pt_g, tab, pj.npts, pj.ch_scale,
-                                                   coef, pj.na * NCH);
-}
-
-template <typename T, int NCH>
-static void launch_project_chunk_nch(const DevProjectors& pj, int cn, const T* X, long long ldx, T* coef,
-                                     cudaStream_t st) {
-    if (cn > 8) launch_project_chunk_sb<T, 16, NCH>(pj, cn, X, ldx, coef, st);
-    else if (cn > 4) launch_project_chunk_sb<T, 8, NCH>(pj, cn, X, ldx, coef, st);
-    else if (cn > 2) launch_project_chunk_sb<T, 4, NCH>(pj, cn, X, ldx, coef, st);
-    else if (cn > 1) launch_project_chunk_sb<T, 2, NCH>(pj, cn, X, ldx, coef, st);
-    else launch_project_chunk_sb<T, 1, NCH>(pj, cn, X, ldx, coef, st);
-}
-
-template <typename T>
-static int launch_project_chunk(const DevProjectors& pj, int cn, const T* X, long long ldx, T* coef,
-                                cudaStream_t st) {
-    switch (pj.nch) {
-        case 4: launch_project_chunk_nch<T, 4>(pj, cn, X, ldx, coef, st); return QG_OK;
-        case 8: launch_project_chunk_nch<T, 8>(pj, cn, X, ldx, coef, st); return QG_OK;
-        case 16: launch_project_chunk_nch<T, 16>(pj, cn, X, ldx, coef, st); return QG_OK;
-        default: return QG_ERR_UNSUPPORTED;
-    }
-}
-
-template <typename T, int C, int NCH>
-static int launch_scatter_c(const DevProjectors& pj, T* HX, long long ldhx, int cn, long long N, const T* coef,
-                            cudaStream_t st) {
-    const T* ev;
-    if constexpr (sizeof(T) == 8) ev = reinterpret_cast<const T*>(pj.ent_val_d);
-    else ev = reinterpret_cast<const T*>(pj.ent_val_f);
-    const size_t smem = (size_t)cn * pj.na * NCH * sizeof(T);
-    auto kern = k_scatter<T, C, NCH>;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return QG_ERR_UNSUPPORTED;
-    const int threads = 256;
-    kern<<<(unsigned)((N + threads - 1) / threads), threads, smem, st>>>(HX, ldhx, cn, N, pj.row, pj.ent_atom, ev,
-                                                                        coef, pj.na * NCH);
-    return QG_OK;
-}
-
-template <typename T, int NCH>
-static int launch_scatter_nch(const DevProjectors& pj, T* HX, long long ldhx, int cn, long long N, const T* coef,
-                              cudaStream_t st) {
-    if (cn > 8) return launch_scatter_c<T, 16, NCH>(pj, HX, ldhx, cn, N, coef, st);
-    if (cn > 4) return launch_scatter_c<T, 8, NCH>(pj, HX, ldhx, cn, N, coef, st);
-    if (cn > 2) return launch_scatter_c<T, 4, NCH>(pj, HX, ldhx, cn, N, coef, st);
-    if (cn > 1) return launch_scatter_c<T, 2, NCH>(pj, HX, ldhx, cn, N, coef, st);
-    return launch_scatter_c<T, 1, NCH>(pj, HX, ldhx, cn, N, coef, st);
-}
-
-template <typename T>
-static int launch_scatter(const DevProjectors& pj, T* HX, long long ldhx, int cn, long long N, const T* coef,
-                          int /*C*/, cudaStream_t st) {
-    switch (pj.nch) {
-        case 4: return launch_scatter_nch<T, 4>(pj, HX, ldhx, cn, N, coef, st);
-        case 8: return launch_scatter_nch<T, 8>(pj, HX, ldhx, cn, N, coef, st);
-        case 16: return launch_scatter_nch<T, 16>(pj, HX, ldhx, cn, N, coef, st);
-        default: return QG_ERR_UNSUPPORTED;
-    }
-}
-
-// Creates the pipeline's side streams and enough events for ns states.
-int ensure_side_streams(qg_hamiltonian h, int ns) {
-    for (int i = 0; i < 2; ++i)
-        if (!h->side[i]) QG_CUDA_TRY(cudaStreamCreateWithFlags(&h->side[i], cudaStreamNonBlocking));
-    const size_t need = 4 + 3 * (size_t)ns;
-    while (h->evs.size() < need) {
-        cudaEvent_t e;
-        QG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        h->evs.push_back(e);
-    }
-    return QG_OK;
-}
-
-// Issues the chunked pipeline. sP runs projection + reduction, sS the stencil,
-// sC the scatter; with three distinct streams consecutive chunks overlap
-// (projection of chunk c+1 next to the stencil of c and the scatter of c-1),
-// with one stream everything is serial (used with phase timing).
-template <typename T>
-int issue_chunks(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx, T* coef,
-                 const HamArgs<T>& a, cudaStream_t sP, cudaStream_t sS, cudaStream_t sC, PhaseTimer* pt) {
-    const DevProjectors& pj = h->pj;
-    const long long N = h->N();
-    const int C = chunk_states(N, sizeof(T));
-    const int ncoef = pj.na * pj.nch;
-    const bool multi = (sP != sS);
-    int ei = 0;
-    auto ev = [&]() { return h->evs[ei++]; };
-    if (multi) {
-        cudaEvent_t fork = ev();
-        QG_CUDA_TRY(cudaEventRecord(fork, sS));
-        QG_CUDA_TRY(cudaStreamWaitEvent(sP, fork, 0));
-        QG_CUDA_TRY(cudaStreamWaitEvent(sC, fork, 0));
-    }
-    T* part = coef + (size_t)ns * ncoef;  // per-split partials of one chunk, reused in stream order on sP
-    for (int c0 = 0; c0 < ns; c0 += C) {
-        const int cn = std::min(C, ns - c0);
-        T* cf = coef + (size_t)c0 * ncoef;
-        if (pt) pt->mark(0, sP);
-        QG_TRY(launch_project_chunk<T>(pj, cn, X + (long long)c0 * ldx, ldx, part, sP));
-        {
-            const int n = cn * ncoef;
-            k_coef_reduce<T><<<(n + 255) / 256, 256, 0, sP>>>(part, cf, n, project_splits(pj));
-        }
-        cudaEvent_t eP = nullptr;
-        if (multi) {
-            eP = ev();
-            QG_CUDA_TRY(cudaEventRecord(eP, sP));
-            QG_CUDA_TRY(cudaStreamWaitEvent(sS, eP, 0));  // the stencil reads psi the projection just pulled into L2
-        }
-        if (pt) pt->mark(1, sS);
-        HamArgs<T> b = a;
-        b.X = X + (long long)c0 * ldx;
-        b.HX = HX + (long long)c0 * ldhx;
-        b.ns = cn;
-        QG_TRY(launch_stencil_tma<T>(b, h->order, sS));
-        if (multi) {
-            cudaEvent_t eS = ev();
-            QG_CUDA_TRY(cudaEventRecord(eS, sS));
-            QG_CUDA_TRY(cudaStreamWaitEvent(sC, eS, 0));
-            QG_CUDA_TRY(cudaStreamWaitEvent(sC, eP, 0));
-        }
-        if (pt) pt->mark(2, sC);
-        QG_TRY(launch_scatter<T>(pj, HX + (long long)c0 * ldhx, ldhx, cn, N, cf, C, sC));
-    }
-    if (pt) pt->mark(-1, sC);
-    if (multi) {
-        cudaEvent_t jP = ev(), jC = ev();
-        QG_CUDA_TRY(cudaEventRecord(jP, sP));
-        QG_CUDA_TRY(cudaEventRecord(jC, sC));
-        QG_CUDA_TRY(cudaStreamWaitEvent(sS, jP, 0));
-        QG_CUDA_TRY(cudaStreamWaitEvent(sS, jC, 0));
-    }
-    return QG_OK;
+    return (size_t)ns * pj.na * pj.nch;
 }
 
 template <typename T>
@@ -896,10 +611,6 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
 
 void destroy_ham(qg_hamiltonian h) {
     if (!h) return;
-    if (h->graph.exec) cudaGraphExecDestroy(h->graph.exec);
-    for (auto e : h->evs) cudaEventDestroy(e);
-    for (int i = 0; i < 2; ++i)
-        if (h->side[i]) cudaStreamDestroy(h->side[i]);
     cudaFree(h->V_d);
     cudaFree(h->V_f);
     free_projectors(h->pj);
@@ -977,7 +688,7 @@ static int apply_device(qg_hamiltonian h, int ns, const T* X, long long ldx, T* 
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     T* coef = nullptr;
     if (h->pj.na > 0) {
-        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, ns, sizeof(T)) * sizeof(T)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, ns) * sizeof(T)));
         coef = h->coef.as<T>();
     }
     return qg::apply_hamiltonian<T>(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream);
@@ -1003,7 +714,7 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     double* coef = nullptr;
     if (h->pj.na > 0) {
-        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, ns, sizeof(double)) * sizeof(double)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, ns) * sizeof(double)));
         coef = h->coef.as<double>();
     }
     qg::PhaseTimer pt;

@@ -88,18 +88,6 @@ struct qg_hamiltonian_s {
     DevBuf xio, hxio; // staging for the host-buffer entry point
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
-    int use_graph = 1;            // replay the chunked pipeline from a captured CUDA graph
-    cudaStream_t side[2] = {nullptr, nullptr};  // projection and scatter streams of the pipeline
-    std::vector<cudaEvent_t> evs;               // pipeline events (timing disabled)
-    struct GraphCache {
-        cudaGraphExec_t exec = nullptr;
-        int ns = 0, dtype = 0;
-        const void* X = nullptr;
-        void* HX = nullptr;
-        long long ldx = 0, ldhx = 0;
-        cudaStream_t st = nullptr;
-        const void* coef = nullptr;
-    } graph;
     long long N() const { return (long long)nx * ny * nz; }
 };
 
@@ -136,10 +124,8 @@ struct PhaseTimer {
     }
 };
 
-int chunk_states(long long N, size_t elem);
-int project_splits(const DevProjectors& pj);
-// Elements of projector-coefficient scratch one apply of ns states needs.
-size_t coef_scratch_elems(qg_hamiltonian h, int ns, size_t elem);
+// Elements of projector-coefficient scratch ([ns][n_atoms * n_channels]) one apply of ns states needs.
+size_t coef_scratch_elems(qg_hamiltonian h, int ns);
 
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,

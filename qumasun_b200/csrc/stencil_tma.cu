@@ -1,18 +1,18 @@
-// Fused FD stencil + local potential (+ optional per-point nonlocal scatter),
-// TMA-staged and warp-specialised (sm_100a).
+// FD stencil + local potential, H psi = V psi - 1/2 Lap psi, as a persistent,
+// TMA-staged, warp-specialised kernel (sm_100a).
 //
-// Same operator as k_hamiltonian (hamiltonian.cu), organised for bandwidth:
-//  * one thread block = SPB states x (ty full x-rows) x a slab of z planes;
-//  * warp 0 is the producer: one lane streams every plane the block needs
-//    (ty + 2R rows: the y halo rows ride in the same copy, split where the tile
-//    wraps periodically in y) into a ring of `nst` shared-memory stages with
-//    bulk async copies (cp.async.bulk), completion counted on a "full" mbarrier
-//    per stage and state;
+//  * one block per SM loops over work items (state, y tile of ty full x-rows,
+//    z slab); the plane ring and its mbarrier phases run on across items, so the
+//    pipeline never drains between items;
+//  * warp 0 is the producer: one lane streams every plane an item needs (ty + 2R
+//    rows: the y halo rows ride in the same copy, split where the tile wraps
+//    periodically in y) into a ring of `nst` shared-memory stages with bulk async
+//    copies (cp.async.bulk), completion counted on a "full" mbarrier per stage;
 //  * the other warps are consumers: each thread owns PX consecutive x-points
 //    (one 16-byte vector) of one row, keeps their 2R+1 z-values in registers
 //    (filled from the ring), reads x and y neighbours from the stage of the
-//    current plane with 16-byte shared loads (x wraps by index), prefetches
-//    V R steps ahead into registers, and writes H psi with 16-byte stores;
+//    current plane with 16-byte shared loads (x wraps by index), prefetches V
+//    R planes ahead into registers, and writes H psi with 16-byte stores;
 //  * a consumer warp releases a stage by arriving on its "empty" mbarrier once
 //    its reads of that plane are done; the producer refills a stage only after
 //    every consumer warp released it. No block-wide barrier per plane.
@@ -121,10 +121,8 @@ __device__ __forceinline__ T lap_point(T c, const T* xm, const T* xp, const T* y
 }
 
 constexpr int kBarBytes = 1024;  // mbarriers + control words at the front of dynamic shared memory
-constexpr int kMaxThreads = 512;
-constexpr int kMaxConsumers = 352;
-constexpr int kNlWarps = 4;      // warps computing the per-point nonlocal sums
-constexpr int kNlStages = 4;     // planes of nonlocal sums in flight
+constexpr int kMaxThreads = 416;
+constexpr int kMaxConsumers = 384;
 constexpr int kMaxStages = 16;
 
 template <int ORDER>
@@ -141,7 +139,7 @@ struct WorkGrid {
 // item = (state, y tile, z slab). The plane ring and its phases run on across
 // items, so the producer streams the next item's planes while the consumers
 // finish the current one.
-template <typename T, int ORDER, int PX, bool NL>
+template <typename T, int ORDER, int PX>
 __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T> a, const WorkGrid wg, int nst) {
     constexpr int R = radius<ORDER>();
     constexpr int Q = 2 * R + 1;
@@ -150,9 +148,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);               // [nst]
     uint64_t* empty = full + nst;                                      // [nst]
-    uint64_t* nlfull = empty + nst;                                    // [kNlStages]
-    uint64_t* nlempty = nlfull + kNlStages;                            // [kNlStages]
-    volatile int* ctl = reinterpret_cast<volatile int*>(nlempty + kNlStages);  // [0] abort, [1] last position issued
+    volatile int* ctl = reinterpret_cast<volatile int*>(empty + nst);  // [0] abort, [1] last position issued
     T* ring = reinterpret_cast<T*>(smem + kBarBytes);
 
     const int nx = a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
@@ -162,9 +158,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
     const int tpr = nx / PX;
     const int ncons = tpr * ty;
     const int ncons_warps = (ncons + 31) / 32;
-    const int nl_start = 32 + 32 * ncons_warps;  // first thread of the nonlocal warps
-    const int tile_pts = ty * nx;
-    T* nlring = ring + (size_t)nst * stage_elems;  // [kNlStages][ty*nx] per-point nonlocal sums
     const int t = threadIdx.x;
     const long long plane = (long long)nx * ny;
 
@@ -172,10 +165,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
         for (int i = 0; i < nst; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], (uint32_t)ncons_warps);
-        }
-        for (int i = 0; i < kNlStages; ++i) {
-            mbar_init(&nlfull[i], (uint32_t)kNlWarps);
-            mbar_init(&nlempty[i], (uint32_t)ncons_warps);
         }
         ctl[0] = 0;
         ctl[1] = -1;
@@ -219,64 +208,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
                 }
             }
         }
-    } else if (NL && t >= nl_start) {
-        // ---------------- nonlocal warps: per-point projector scatter sums, planes ahead ----------------
-        const int lane = t & 31;
-        const int u = t - nl_start;
-        int k = 0;
-        uint32_t ph = 0;
-        int npos = 0;
-        for (int item = blockIdx.x; item < wg.items && !ctl[0]; item += gridDim.x) {
-            const int slab = item % wg.nslab;
-            const int tile = (item / wg.nslab) % wg.tiles;
-            const int s = item / (wg.nslab * wg.tiles);
-            const int zs = slab * wg.zslab;
-            const int ze = min(nz, zs + wg.zslab);
-            const T* cf = a.coef + (long long)s * a.ncoef;
-            const long long gbase = (long long)tile * tile_pts;
-            bool stop = false;
-            for (int z = zs; z < ze; ++z, ++npos) {
-                if (npos >= kNlStages && !mbar_wait(&nlempty[k], ph ^ 1u)) {
-                    ctl[0] = 1;
-                    atomicExch(a.err, (int)QG_ERR_TIMEOUT);
-                    stop = true;
-                }
-                if (__any_sync(0xffffffffu, stop || ctl[0] != 0)) {
-                    stop = true;
-                    break;
-                }
-                T* dst = nlring + (size_t)k * tile_pts;
-                const long long g0 = (long long)z * plane + gbase;
-                for (int p = u; p < tile_pts; p += 32 * kNlWarps * 2) {
-                    // two points per iteration: both entry ranges are fetched before either is walked
-                    const int p2 = p + 32 * kNlWarps;
-                    const bool has2 = p2 < tile_pts;
-                    const int e0 = a.row[g0 + p], e1 = a.row[g0 + p + 1];
-                    int f0 = 0, f1 = 0;
-                    if (has2) {
-                        f0 = a.row[g0 + p2];
-                        f1 = a.row[g0 + p2 + 1];
-                    }
-                    T acc = T(0), acc2 = T(0);
-                    for (int e = e0; e < e1; ++e) {
-                        const T* ev = a.ent_val + (long long)e * a.nch;
-                        const T* cc = cf + a.ent_atom[e] * a.nch;
-                        for (int ch = 0; ch < a.nch; ++ch) acc += ev[ch] * cc[ch];
-                    }
-                    for (int e = f0; e < f1; ++e) {
-                        const T* ev = a.ent_val + (long long)e * a.nch;
-                        const T* cc = cf + a.ent_atom[e] * a.nch;
-                        for (int ch = 0; ch < a.nch; ++ch) acc2 += ev[ch] * cc[ch];
-                    }
-                    dst[p] = acc;
-                    if (has2) dst[p2] = acc2;
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&nlfull[k]);
-                if (++k == kNlStages) { k = 0; ph ^= 1u; }
-            }
-            if (stop) break;
-        }
     } else if (t < 32 + ncons) {
         // ---------------- consumer warps ----------------
         const unsigned wmask = __activemask();
@@ -296,8 +227,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
             xoff[v] = rowoff + xx;
         }
         int pos = 0;  // ring position of the current item's first plane
-        int nk = 0;   // nonlocal ring stage of the current plane
-        uint32_t nph = 0;
         bool bad = false;
         for (int item = blockIdx.x; item < wg.items && !bad; item += gridDim.x) {
             const int slab = item % wg.nslab;
@@ -342,15 +271,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
             for (int z = zs; z < ze; ++z) {
                 if (z + R < ze) vq[R].v = *reinterpret_cast<const VT*>(vp);
                 vp += plane;
-                bool ok = mbar_wait(&full[jp], php);
-                Vec<T, PX> nlv;
-                if constexpr (NL) {
-                    if (ok) ok = mbar_wait(&nlfull[nk], nph);
-                    nlv.v = *reinterpret_cast<const VT*>(nlring + (size_t)nk * tile_pts + ly * nx + ix0);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < PX; ++e) nlv.e[e] = T(0);
-                }
+                const bool ok = mbar_wait(&full[jp], php);
                 if (__any_sync(wmask, !ok || ctl[0] != 0)) {
                     bad = true;
                     break;
@@ -376,13 +297,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
                     ymv[d - 1].v = *reinterpret_cast<const VT*>(pzs + rowoff + ix0 - d * nx);
                 }
                 __syncwarp(wmask);
-                if (lane == 0) {
-                    mbar_arrive(&empty[jz]);  // plane z is no longer read
-                    if constexpr (NL) mbar_arrive(&nlempty[nk]);
-                }
-                if constexpr (NL) {
-                    if (++nk == kNlStages) { nk = 0; nph ^= 1u; }
-                }
+                if (lane == 0) mbar_arrive(&empty[jz]);  // plane z is no longer read
                 Vec<T, PX> out;
 #pragma unroll
                 for (int e = 0; e < PX; ++e) {
@@ -398,7 +313,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
                     }
                     const T cc = q[R].e[e];
                     const T lap = lap_point<T, ORDER>(cc, xm, xp, ym, yp, zm, zp, a);
-                    out.e[e] = (vq[0].e[e] * cc + nlv.e[e]) + lap;
+                    out.e[e] = vq[0].e[e] * cc + lap;
                 }
                 *reinterpret_cast<VT*>(hxp) = out.v;
                 hxp += plane;
@@ -441,9 +356,9 @@ int tma_tile_rows(const HamArgs<T>& a) {
     return ty;
 }
 
-// Ring stages that fit next to the nonlocal ring (nl_bytes) in the shared-memory budget.
-int ring_stages_for(int R, size_t stage_bytes, size_t nl_bytes = 0) {
-    const size_t budget = 200 * 1024 - kBarBytes - nl_bytes;
+// Ring stages that fit the shared-memory budget.
+int ring_stages_for(int R, size_t stage_bytes) {
+    const size_t budget = 200 * 1024 - kBarBytes;
     int nst = (int)std::min<size_t>(kMaxStages, budget / stage_bytes);
     const int need = std::max(2 * R, R + 2);
     return nst >= need ? nst : -1;
@@ -460,20 +375,19 @@ int sm_count() {
     return n;
 }
 
-template <typename T, int ORDER, bool NL>
-int launch_order_nl(const HamArgs<T>& a, cudaStream_t st) {
+template <typename T, int ORDER>
+int launch_order(const HamArgs<T>& a, cudaStream_t st) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = radius<ORDER>();
     const size_t stage = (size_t)(a.ty + 2 * R) * a.nx * sizeof(T);
-    const size_t nl_bytes = NL ? (size_t)kNlStages * a.ty * a.nx * sizeof(T) : 0;
-    const int nst = ring_stages_for(R, stage, nl_bytes);
+    const int nst = ring_stages_for(R, stage);
     if (nst < 0) return QG_ERR_UNSUPPORTED;
-    const size_t smem = kBarBytes + (size_t)nst * stage + nl_bytes;
-    auto kern = k_stencil_tma<T, ORDER, PX, NL>;
+    const size_t smem = kBarBytes + (size_t)nst * stage;
+    auto kern = k_stencil_tma<T, ORDER, PX>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * a.ty;
-    const int threads = 32 + 32 * ((ncons + 31) / 32) + (NL ? 32 * kNlWarps : 0);
+    const int threads = 32 + ncons;
     if (threads > kMaxThreads) return QG_ERR_UNSUPPORTED;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
@@ -493,26 +407,20 @@ int launch_order_nl(const HamArgs<T>& a, cudaStream_t st) {
     return QG_OK;
 }
 
-template <typename T, int ORDER>
-int launch_order(const HamArgs<T>& a, cudaStream_t st) {
-    if (a.row) return launch_order_nl<T, ORDER, true>(a, st);
-    return launch_order_nl<T, ORDER, false>(a, st);
-}
-
 }  // namespace
 
 template <typename T>
 bool stencil_tma_ok(const HamArgs<T>& a, int order) {
     constexpr int PX = 16 / sizeof(T);
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
+    if (a.row) return false;  // the nonlocal scatter runs in k_scatter_all on this path
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R)
         return false;
     const int ty = tma_tile_rows(a);
     if (ty == 0) return false;
     const size_t stage = (size_t)(ty + 2 * R) * a.nx * sizeof(T);
-    const size_t nl_bytes = (size_t)kNlStages * ty * a.nx * sizeof(T);  // sized as if the nonlocal term is on
-    return ring_stages_for(R, stage, nl_bytes) > 0;
+    return ring_stages_for(R, stage) > 0;
 }
 
 // Returns QG_ERR_UNSUPPORTED (launching nothing) when the shape or alignment
