@@ -90,6 +90,8 @@ def lib():
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_set_stencil_kernel.argtypes = [vp, C.c_int]
         L.qg_context_take_device_status.argtypes = [vp]
+        L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
+        L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         _lib = L
     return _lib
 
@@ -197,6 +199,15 @@ class Hamiltonian:
             raise TypeError("states must be float64 or float32")
         self.ctx.use_torch_stream()
         self.apply_device(X.shape[0], X.data_ptr(), out.data_ptr(), dtype=dt)
+        return out
+
+    def apply_noalloc(self, X, out):
+        """HX = H X (FP64 torch CUDA tensors) through the entry point that allocates
+        nothing: the projector coefficients use the library's fixed scratch array."""
+        self.ctx.use_torch_stream()
+        check(lib().qg_hamiltonian_apply_noalloc_d(self.h, X.shape[0], C.c_void_p(X.data_ptr()), self.N,
+                                                   C.c_void_p(out.data_ptr()), self.N),
+              "qg_hamiltonian_apply_noalloc_d")
         return out
 
     def apply_timed(self, ns, x_ptr, hx_ptr):
