@@ -149,6 +149,42 @@ int qg_hamiltonian_apply_noalloc_d(qg_hamiltonian ham, int ns, const double* X, 
 /* Capacity, in doubles, of the fixed scratch array qg_hamiltonian_apply_noalloc_d uses. */
 size_t qg_noalloc_scratch_capacity(void);
 
+/* ---- LOBPCG ------------------------------------------------------------ */
+typedef struct qg_lobpcg_options {
+    int max_iter;       /* iteration limit (reference: iter_max) */
+    double tol;         /* stop when max_j sum_i r_j(i)^2 dV < tol * dV (reference limit 1e-10,
+                           lobpcg_d_multi.h:54, :525); <= 0 selects 1e-10 */
+    int first_call;     /* 1: start with P = 0 and the 2n x 2n first step (reference is_first_time) */
+    int precision;      /* QG_FP64: FP64 throughout */
+    int verbose;        /* 1: print (iteration, max residual) lines to stdout */
+} qg_lobpcg_options;
+
+typedef struct qg_lobpcg_report {
+    int iterations;     /* LOBPCG iterations taken (H applications to R) */
+    int converged;      /* 1 if the residual criterion was met */
+    double max_residual;/* max_j sum_i r_j(i)^2 dV at exit */
+    double ms_total;    /* device time of the solve */
+    double ms_hamiltonian, ms_gram, ms_eigensolve, ms_rotate, ms_vector;  /* per-phase device time */
+} qg_lobpcg_report;
+
+/* Block LOBPCG for the ns lowest eigenpairs of H, FP64 on the GPU.
+ * Replaces EigenLOBPCG_d_multi (lobpcg_d_multi.h:23-545): same iteration (x
+ * normalised with dV, residual r = Ax - (x.Ax dV) x, the 3n x 3n pencil
+ * ([x r p]^T [Ax Ar Ap] dV, [x r p]^T [x r p] dV) -- 2n x 2n on the first step --
+ * solved for its ns lowest pairs, P = R Cr + P Cp, X = X Cx + P, columns
+ * renormalised, same stopping rule), with the Gram and rotation products as
+ * DGEMMs (the w_dgemm path of lobpcg_d_multi_mpi.h:191-579) and the small
+ * generalised eigenproblem solved on the GPU (replaces lapack_DSYGVX,
+ * w_dsygvx.h:24-104). X (ns*N, in/out), P (ns*N, in/out, the reference's
+ * "keep") and ev (ns, out) are HOST buffers, state-major. Returns
+ * QG_ERR_NOT_CONVERGED (results still written) when max_iter is reached,
+ * QG_ERR_CHOLESKY if the Gram matrix of [x r p] is not positive definite. */
+int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
+                double* P, qg_lobpcg_report* report);
+/* Same with DEVICE buffers X and P (ld = N); ev stays a host array. */
+int qg_lobpcg_d_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
+                       double* X, double* P, qg_lobpcg_report* report);
+
 /* Selects the stencil kernel of an operator: 0 = the TMA-staged ring kernel
  * where the shape and alignment allow (default), 1 = always the
  * register-window kernel (any shape). Both compute the same operator. */

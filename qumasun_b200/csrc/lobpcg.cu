@@ -1,0 +1,398 @@
+// Block LOBPCG on the GPU, FP64 (EigenLOBPCG_d_multi, lobpcg_d_multi.h:23-545).
+//
+// Blocks live on the device as column-major N x n arrays (= the reference's
+// state-major layout, one state per column):
+//   W  = [x | r | p]      (3n columns, contiguous)
+//   AW = [Ax | Ar | Ap]
+//   T  = [x_new | p_new], AT = [Ax_new | Ap_new] (rotation outputs)
+// One iteration:
+//   Ar = H r                                       (qg::apply_hamiltonian)
+//   Sa = W^T AW dV, Sb = W^T W dV                  (DGEMM; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
+//   Sa z = lambda Sb z, k = 3n (2n on the first step of a first call)   (cusolverDnDsygvd;
+//                                                   replaces DSYGVX, w_dsygvx.h:24-104, UPLO as the reference)
+//   p_new = [r p] [Cr; Cp], x_new = [x r p] [Cx; Cr; Cp] (DGEMM; lobpcg_d_multi.h:247-300)
+//   renormalise x, Ax by |x|, p, Ap by |p| (:491-505); ei = x.Ax dV; r = Ax - ei x (:506-512)
+//   stop when max_j sum r_j^2 dV < tol dV (:525).
+// Column reductions (norms, dots, residuals) are project kernels with one
+// block per column and a fixed reduction order (deterministic).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "qg_internal.h"
+
+#define QG_BLAS_TRY(expr)                                                                   \
+    do {                                                                                    \
+        cublasStatus_t qg_b_ = (expr);                                                      \
+        if (qg_b_ != CUBLAS_STATUS_SUCCESS) {                                               \
+            char m_[32];                                                                    \
+            snprintf(m_, sizeof(m_), "cublas status %d", (int)qg_b_);                       \
+            qg_set_last_error(#expr, m_, __FILE__, __LINE__);                               \
+            return QG_ERR_LIBRARY;                                                          \
+        }                                                                                   \
+    } while (0)
+
+#define QG_SOLVER_TRY(expr)                                                                 \
+    do {                                                                                    \
+        cusolverStatus_t qg_v_ = (expr);                                                    \
+        if (qg_v_ != CUSOLVER_STATUS_SUCCESS) {                                             \
+            char m_[32];                                                                    \
+            snprintf(m_, sizeof(m_), "cusolver status %d", (int)qg_v_);                     \
+            qg_set_last_error(#expr, m_, __FILE__, __LINE__);                               \
+            return QG_ERR_LIBRARY;                                                          \
+        }                                                                                   \
+    } while (0)
+
+int qg_blas_handle(qg_context c, cublasHandle_t* out) {
+    if (!c->blas) {
+        cublasHandle_t h;
+        QG_BLAS_TRY(cublasCreate(&h));
+        c->blas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->blas);
+    QG_BLAS_TRY(cublasSetStream(h, c->stream));
+    QG_BLAS_TRY(cublasSetMathMode(h, CUBLAS_DEFAULT_MATH));
+    *out = h;
+    return QG_OK;
+}
+
+int qg_solver_handle(qg_context c, cusolverDnHandle_t* out) {
+    if (!c->solver) {
+        cusolverDnHandle_t h;
+        QG_SOLVER_TRY(cusolverDnCreate(&h));
+        c->solver = h;
+    }
+    cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(c->solver);
+    QG_SOLVER_TRY(cusolverDnSetStream(h, c->stream));
+    *out = h;
+    return QG_OK;
+}
+
+namespace {
+
+constexpr int kRedThreads = 512;
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double red[kRedThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    }
+    return s;  // valid in thread 0
+}
+
+// out[j] = scale * sum_i A[j][i] * B[j][i]
+__global__ void __launch_bounds__(kRedThreads) k_coldot(const double* __restrict__ A, const double* __restrict__ B,
+                                                        long long ld, long long N, double scale,
+                                                        double* __restrict__ out) {
+    const double* a = A + (long long)blockIdx.x * ld;
+    const double* b = B + (long long)blockIdx.x * ld;
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < N; i += blockDim.x) s += a[i] * b[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[blockIdx.x] = s * scale;
+}
+
+// A[j][:] *= f[j] for the columns of up to two blocks sharing the factors
+__global__ void k_scale_cols(double* __restrict__ A, double* __restrict__ B, long long ld, long long N,
+                             const double* __restrict__ f) {
+    const int j = blockIdx.y;
+    const double c = f[j];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        A[(long long)j * ld + i] *= c;
+        if (B) B[(long long)j * ld + i] *= c;
+    }
+}
+
+// f[j] = 1 / sqrt(norm2[j] * dV)   (Normalize, vecmath.h:128-133)
+__global__ void k_inv_norm(const double* __restrict__ norm2, double dV, int n, double* __restrict__ f) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) f[j] = 1.0 / sqrt(norm2[j] * dV);
+}
+
+// r_j = Ax_j - ei_j x_j and nr[j] = dV * sum_i r_j(i)^2   (lobpcg_d_multi.h:506-516)
+__global__ void __launch_bounds__(kRedThreads) k_residual(const double* __restrict__ Ax, const double* __restrict__ x,
+                                                          const double* __restrict__ ei, double* __restrict__ r,
+                                                          long long ld, long long N, double dV,
+                                                          double* __restrict__ nr) {
+    const long long off = (long long)blockIdx.x * ld;
+    const double e = ei[blockIdx.x];
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < N; i += blockDim.x) {
+        const double v = Ax[off + i] - e * x[off + i];
+        r[off + i] = v;
+        s += v * v;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) nr[blockIdx.x] = s * dV;
+}
+
+struct Timer {
+    cudaEvent_t ev[8];
+    int n = 0;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    int tag[8];
+    bool ok = true;
+    Timer() {
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess) ok = false;
+    }
+    ~Timer() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+    void mark(int t, cudaStream_t st) {
+        if (n < 8) {
+            cudaEventRecord(ev[n], st);
+            tag[n++] = t;
+        }
+    }
+    void flush() {  // call after the stream has reached the last mark
+        for (int i = 0; i + 1 < n; ++i) {
+            float d = 0.f;
+            cudaEventElapsedTime(&d, ev[i], ev[i + 1]);
+            if (tag[i] >= 0 && tag[i] < 6) acc[tag[i]] += d;
+        }
+        n = 0;
+    }
+};
+
+struct Solver {
+    qg_hamiltonian h;
+    int n;
+    long long N;
+    double dV;
+    cudaStream_t st;
+    cublasHandle_t blas;
+    cusolverDnHandle_t sol;
+    DevBuf W, AW, T, AT, S, small, work;
+    int lwork = 0;
+    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb;
+    double *ev_d, *nr_d, *f_d, *f2_d, *w_d;
+    int* info_d;
+
+    ~Solver() {
+        W.release(); AW.release(); T.release(); AT.release(); S.release(); small.release(); work.release();
+    }
+
+    int setup() {
+        const size_t blk = (size_t)N * n;
+        QG_TRY(W.reserve(3 * blk * sizeof(double)));
+        QG_TRY(AW.reserve(3 * blk * sizeof(double)));
+        QG_TRY(T.reserve(2 * blk * sizeof(double)));
+        QG_TRY(AT.reserve(2 * blk * sizeof(double)));
+        const size_t k3 = 3 * (size_t)n;
+        QG_TRY(S.reserve(2 * k3 * k3 * sizeof(double)));
+        QG_TRY(small.reserve((5 * k3 + 16) * sizeof(double)));
+        x = W.as<double>(); r = x + blk; p = r + blk;
+        Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
+        Tx = T.as<double>(); Tp = Tx + blk;
+        ATx = AT.as<double>(); ATp = ATx + blk;
+        Sa = S.as<double>(); Sb = Sa + k3 * k3;
+        ev_d = small.as<double>(); nr_d = ev_d + k3; f_d = nr_d + k3; f2_d = f_d + k3; w_d = f2_d + k3;
+        info_d = reinterpret_cast<int*>(w_d + k3);
+        QG_SOLVER_TRY(cusolverDnDsygvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                  CUBLAS_FILL_MODE_LOWER, (int)k3, Sa, (int)k3, Sb, (int)k3, w_d,
+                                                  &lwork));
+        QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(double)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, n) * sizeof(double)));
+        return QG_OK;
+    }
+
+    int applyH(const double* in, double* out) {
+        return qg::apply_hamiltonian<double>(h, n, in, N, out, N, h->coef.as<double>(), st);
+    }
+
+    void coldot(const double* A, const double* B, double scale, double* out) {
+        k_coldot<<<n, kRedThreads, 0, st>>>(A, B, N, N, scale, out);
+    }
+
+    // scale columns of A (and B) by 1/sqrt(|A_j|^2 dV) computed from A
+    void normalize(double* A, double* B) {
+        coldot(A, A, 1.0, nr_d);
+        k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(nr_d, dV, n, f_d);
+        dim3 g((unsigned)std::min<long long>((N + 255) / 256, 64), n);
+        k_scale_cols<<<g, 256, 0, st>>>(A, B, N, N, f_d);
+    }
+
+    // C (m x nn, ldc) = alpha * A^T B, A: N x m, B: N x nn (ld N)
+    int gemm_tn(int m, int nn, const double* A, const double* B, double alpha, double* C, int ldc) {
+        const double beta = 0.0;
+        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, nn, (int)N, &alpha, A, (int)N, B, (int)N, &beta,
+                                C, ldc));
+        return QG_OK;
+    }
+
+    // C (N x n) = A (N x k) * Z (k x n, ldz)
+    int gemm_nn(int k, const double* A, const double* Z, int ldz, double* C) {
+        const double one = 1.0, zero = 0.0;
+        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, n, k, &one, A, (int)N, Z, ldz, &zero, C,
+                                (int)N));
+        return QG_OK;
+    }
+};
+
+int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev, double* X_dev, double* P_dev,
+               const double* X_host, double* Xout_host, const double* P_host, double* Pout_host,
+               qg_lobpcg_report* rep) {
+    if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
+    if (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0) return QG_ERR_INVALID;
+    if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
+    const long long N = h->N();
+    if ((long long)n * 3 > N) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    Solver s;
+    s.h = h;
+    s.n = n;
+    s.N = N;
+    s.dV = h->hx * h->hy * h->hz;
+    s.st = h->ctx->stream;
+    QG_TRY(qg_blas_handle(h->ctx, &s.blas));
+    QG_TRY(qg_solver_handle(h->ctx, &s.sol));
+    QG_TRY(s.setup());
+    const size_t blk_bytes = (size_t)N * n * sizeof(double);
+    const bool first = opt->first_call != 0;
+    const double tol = opt->tol > 0 ? opt->tol : 1.0e-10;
+    cudaStream_t st = s.st;
+    Timer tm;
+    cudaEvent_t t0, t1;
+    QG_CUDA_TRY(cudaEventCreate(&t0));
+    QG_CUDA_TRY(cudaEventCreate(&t1));
+    QG_CUDA_TRY(cudaEventRecord(t0, st));
+
+    // inputs
+    if (X_host) QG_CUDA_TRY(cudaMemcpyAsync(s.x, X_host, blk_bytes, cudaMemcpyHostToDevice, st));
+    else QG_CUDA_TRY(cudaMemcpyAsync(s.x, X_dev, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    if (first) {
+        QG_CUDA_TRY(cudaMemsetAsync(s.p, 0, blk_bytes, st));
+    } else if (P_host) {
+        QG_CUDA_TRY(cudaMemcpyAsync(s.p, P_host, blk_bytes, cudaMemcpyHostToDevice, st));
+    } else {
+        QG_CUDA_TRY(cudaMemcpyAsync(s.p, P_dev, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    }
+
+    // initial residual (lobpcg_d_multi.h:64-91)
+    s.normalize(s.x, nullptr);
+    QG_TRY(s.applyH(s.x, s.Ax));
+    if (first) QG_CUDA_TRY(cudaMemsetAsync(s.Ap, 0, blk_bytes, st));
+    else QG_TRY(s.applyH(s.p, s.Ap));
+    s.coldot(s.x, s.Ax, s.dV, s.ev_d);
+    k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
+    {
+        k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, 1.0, n, s.f_d);
+        dim3 g((unsigned)std::min<long long>((N + 255) / 256, 64), n);
+        k_scale_cols<<<g, 256, 0, st>>>(s.r, nullptr, N, N, s.f_d);
+    }
+    QG_CUDA_TRY(cudaGetLastError());
+
+    std::vector<double> ev_h(n), nr_h(n);
+    int info_h = 0;
+    int it = 0;
+    bool converged = false;
+    double maxres = 0.0;
+    int status = QG_OK;
+    for (it = 0; it < opt->max_iter; ++it) {
+        tm.mark(0, st);
+        QG_TRY(s.applyH(s.r, s.Ar));
+        tm.mark(1, st);
+        const bool two = first && it == 0;
+        const int k3 = (two ? 2 : 3) * n;
+        QG_TRY(s.gemm_tn(k3, k3, s.x, s.Ax, s.dV, s.Sa, k3));
+        QG_TRY(s.gemm_tn(k3, k3, s.x, s.x, s.dV, s.Sb, k3));
+        tm.mark(2, st);
+        QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                       k3, s.Sa, k3, s.Sb, k3, s.w_d, s.work.as<double>(), s.lwork, s.info_d));
+        tm.mark(3, st);
+        // rotation: columns 0..n-1 of Sa are (Cx; Cr; Cp)
+        QG_TRY(s.gemm_nn(k3 - n, s.r, s.Sa + n, k3, s.Tp));    // p_new = [r p] [Cr; Cp]
+        QG_TRY(s.gemm_nn(k3 - n, s.Ar, s.Sa + n, k3, s.ATp));
+        QG_TRY(s.gemm_nn(k3, s.x, s.Sa, k3, s.Tx));            // x_new = [x r p] [Cx; Cr; Cp]
+        QG_TRY(s.gemm_nn(k3, s.Ax, s.Sa, k3, s.ATx));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.Ax, s.ATx, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.Ap, s.ATp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        tm.mark(4, st);
+        s.normalize(s.x, s.Ax);
+        s.normalize(s.p, s.Ap);
+        s.coldot(s.x, s.Ax, s.dV, s.ev_d);
+        k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
+        QG_CUDA_TRY(cudaGetLastError());
+        QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(&info_h, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+        tm.mark(5, st);
+        tm.mark(-1, st);
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        tm.flush();
+        if (info_h != 0) {
+            status = info_h > 0 ? QG_ERR_CHOLESKY : QG_ERR_LIBRARY;
+            ++it;
+            break;
+        }
+        maxres = *std::max_element(nr_h.begin(), nr_h.end());
+        if (!std::isfinite(maxres)) {
+            status = QG_ERR_NONFINITE;
+            ++it;
+            break;
+        }
+        if (opt->verbose) printf("lobpcg iter %d max residual %.3e\n", it + 1, maxres);
+        if (maxres < tol * s.dV) {
+            converged = true;
+            ++it;
+            break;
+        }
+    }
+    // outputs
+    QG_CUDA_TRY(cudaMemcpyAsync(ev_h.data(), s.ev_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (Xout_host) QG_CUDA_TRY(cudaMemcpyAsync(Xout_host, s.x, blk_bytes, cudaMemcpyDeviceToHost, st));
+    else QG_CUDA_TRY(cudaMemcpyAsync(X_dev, s.x, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    if (Pout_host) QG_CUDA_TRY(cudaMemcpyAsync(Pout_host, s.p, blk_bytes, cudaMemcpyDeviceToHost, st));
+    else if (P_dev) QG_CUDA_TRY(cudaMemcpyAsync(P_dev, s.p, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    QG_CUDA_TRY(cudaEventRecord(t1, st));
+    QG_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int j = 0; j < n; ++j) ev[j] = ev_h[j];
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rep) {
+        rep->iterations = it;
+        rep->converged = converged ? 1 : 0;
+        rep->max_residual = maxres;
+        rep->ms_total = tot;
+        rep->ms_hamiltonian = tm.acc[0];
+        rep->ms_gram = tm.acc[1];
+        rep->ms_eigensolve = tm.acc[2];
+        rep->ms_rotate = tm.acc[3];
+        rep->ms_vector = tm.acc[4];
+    }
+    const int dstat = qg_context_take_device_status(h->ctx);
+    if (dstat != QG_OK) return dstat;
+    if (status != QG_OK) return status;
+    return converged ? QG_OK : QG_ERR_NOT_CONVERGED;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qg_lobpcg_d(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
+                qg_lobpcg_report* rep) {
+    if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
+    return run_lobpcg(h, opt, ns, ev, nullptr, nullptr, X, X, P, P, rep);
+}
+
+int qg_lobpcg_d_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
+                       qg_lobpcg_report* rep) {
+    if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
+    return run_lobpcg(h, opt, ns, ev, X, P, nullptr, nullptr, nullptr, nullptr, rep);
+}
+
+}  // extern "C"

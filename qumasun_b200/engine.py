@@ -60,6 +60,24 @@ class HamiltonianDesc(C.Structure):
     ]
 
 
+class LobpcgOptions(C.Structure):
+    """qg_lobpcg_options."""
+
+    _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("first_call", C.c_int),
+                ("precision", C.c_int), ("verbose", C.c_int)]
+
+
+class LobpcgReport(C.Structure):
+    """qg_lobpcg_report."""
+
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("max_residual", C.c_double),
+                ("ms_total", C.c_double), ("ms_hamiltonian", C.c_double), ("ms_gram", C.c_double),
+                ("ms_eigensolve", C.c_double), ("ms_rotate", C.c_double), ("ms_vector", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -92,6 +110,9 @@ def lib():
         L.qg_context_take_device_status.argtypes = [vp]
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
+        L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
+        L.qg_lobpcg_d_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
+                                         C.POINTER(LobpcgReport)]
         _lib = L
     return _lib
 
@@ -209,6 +230,21 @@ class Hamiltonian:
                                                    C.c_void_p(out.data_ptr()), self.N),
               "qg_hamiltonian_apply_noalloc_d")
         return out
+
+    def lobpcg(self, X0, max_iter=2000, tol=1.0e-10, P0=None, first=True, verbose=False):
+        """Block LOBPCG (qg_lobpcg_d) from host states X0 (ns, N); returns
+        dict(ev, X, P, report, status). NOT_CONVERGED is reported, not raised."""
+        X = np.ascontiguousarray(X0, dtype=np.float64).copy()
+        ns = X.shape[0]
+        P = np.zeros_like(X) if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).copy()
+        ev = np.zeros(ns)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0)
+        rep = LobpcgReport()
+        st = lib().qg_lobpcg_d(self.h, C.byref(opt), ns, ev.ctypes.data_as(_dp), X.ctypes.data, P.ctypes.data,
+                               C.byref(rep))
+        if st not in (QG_OK, -9):
+            check(st, "qg_lobpcg_d")
+        return dict(ev=ev, X=X, P=P, report=rep.as_dict(), status=st)
 
     def apply_timed(self, ns, x_ptr, hx_ptr):
         """FP64 apply with device phase times (ms): (projection, stencil + V, scatter)."""
