@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 
 NS = 256
 REPS = (2, 2, 2)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_stencil_tma launch per
+# state of this workload, from an ncu --set full capture of the same bench at 32 states
+# (234.6 MB / 32); traffic grows in proportion to the states, so a full launch is scaled.
+STENCIL_DRAM_BYTES_PER_STATE = 234604544 / 32
 FD_ORDER = 8
 WORKLOAD = "diamond64_80cube_Hpsi"
 
@@ -43,6 +47,9 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--sweep", action="store_true", help="also time FD orders 2/4/6 and FP32")
+    p.add_argument("--no-lobpcg", action="store_true", help="skip the LOBPCG time-to-solution leg")
+    p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     return p.parse_args()
 
 
@@ -216,11 +223,57 @@ def run_reference_arm(a):
     return 0
 
 
+def lobpcg_diamond8(ctx, cpu=True):
+    """Time to the 16 lowest eigenpairs of the 8-atom 40^3 cell (FD order 8) from
+    seeded uniform(-0.5, 0.5) states, GPU FP64 LOBPCG, next to the reference's
+    EigenLOBPCG_d_multi timed on a bounded sample of its iterations."""
+    import numpy as np
+    from qumasun_b200 import Hamiltonian
+    from qumasun_b200.cell import build_cell, initial_states
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "lobpcg_diamond8.npz"))
+    cell = build_cell()
+    ns = int(gold["ns"])
+    X0 = initial_states(ns, cell.N, seed=int(gold["seed"]))
+    H = Hamiltonian(ctx, cell)
+    H.lobpcg(X0, max_iter=5)  # warm-up (library handles, workspace)
+    t0 = time.perf_counter()
+    r = H.lobpcg(X0, max_iter=3000)
+    wall = time.perf_counter() - t0
+    H.close()
+    rep = r["report"]
+    out = {"workload": "diamond8_40cube_16states_fd8", "seconds": round(wall, 4),
+           "device_ms": round(rep["ms_total"], 2), "iterations": rep["iterations"],
+           "converged": bool(rep["converged"]),
+           "max_abs_ev_error_vs_reference_Ha": float(np.abs(r["ev"] - gold["ev"]).max()),
+           "phase_ms": {k: round(rep[k], 2) for k in ("ms_hamiltonian", "ms_gram", "ms_eigensolve", "ms_rotate",
+                                                      "ms_vector")},
+           "reference_iterations": int(gold["iters"])}
+    if cpu:
+        try:
+            import oracle as O
+            k = 25
+            t1 = time.perf_counter()
+            rr = O.ref_lobpcg_d_multi(cell, X0, k)
+            per_it = (time.perf_counter() - t1) / max(1, rr["iters"])
+            out["reference_cpu"] = {"seconds_extrapolated": round(per_it * int(gold["iters"]), 2),
+                                    "seconds_per_iteration": round(per_it, 4), "cores": 1,
+                                    "kind": "reference" if O.ref_available() else "port",
+                                    "sample": f"{rr['iters']} iterations of EigenLOBPCG_d_multi, extrapolated to "
+                                              f"the reference's {int(gold['iters'])}"}
+            out["speedup_vs_reference_cpu"] = round(per_it * int(gold["iters"]) / wall, 1)
+        except Exception as ex:
+            out["reference_cpu"] = {"failed": str(ex)}
+    return out
+
+
 # --------------------------------------------------------------- GPU arm
 def run_gpu_arm(a):
     import numpy as np
     import torch
     import torch.distributed as dist
+
+    global NS
+    NS = a.states
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -289,18 +342,21 @@ def run_gpu_arm(a):
     phase_ms = {"projection": round(ms_proj, 4), "stencil_V": round(ms_sten, 4), "scatter": round(ms_scat, 4)}
 
     # e2e through the host-buffer entry point with pinned host states
-    Xh = torch.empty(NS, N, dtype=torch.float64, pin_memory=True)
-    Xh.copy_(X.cpu())
-    HXh = torch.empty_like(Xh).pin_memory()
-    e2e_steps = max(2, min(a.steps, 5))
-    H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())  # warm the staging buffers
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_s = max_over_ranks(e2e_s)
-    e2e_gbs = nbytes * ws / e2e_s / 1e9
+    e2e = None
+    if not a.no_e2e:
+        Xh = torch.empty(NS, N, dtype=torch.float64, pin_memory=True)
+        Xh.copy_(X.cpu())
+        HXh = torch.empty_like(Xh).pin_memory()
+        e2e_steps = max(2, min(a.steps, 5))
+        H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())  # warm the staging buffers
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            H.apply_host_ptr(NS, Xh.data_ptr(), HXh.data_ptr())
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        e2e_s = max_over_ranks(e2e_s)
+        e2e = {"value": round(nbytes * ws / e2e_s / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": NS * N * 8,
+               "d2h_bytes_per_step": NS * N * 8, "seconds_per_step": round(e2e_s, 5)}
 
     sweep = {}
     if a.sweep and rank == 0:
@@ -338,6 +394,10 @@ def run_gpu_arm(a):
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
+    lob = None
+    if rank == 0 and not a.no_lobpcg:
+        lob = lobpcg_diamond8(ctx, cpu=(ws == 1 and not a.no_cpu_baseline))
+
     if rank == 0:
         line = {
             "metric": "H|psi> GB/s (algorithmic)", "value": round(gbs, 2), "unit": "GB/s",
@@ -353,16 +413,19 @@ def run_gpu_arm(a):
                          "frac": round(sten_gbs / peak, 4), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": sten_bytes, "launches": 1,
                          "ms_per_launch": round(ms_sten, 5),
-                         "traffic": None, "phase_ms_per_apply": phase_ms,
+                         "traffic": int(STENCIL_DRAM_BYTES_PER_STATE * NS),
+                         "traffic_note": "ncu capture at 32 states scaled by states",
+                         "phase_ms_per_apply": phase_ms,
                          "whole_apply_frac": round(gbs / peak, 4)},
-            "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": NS * N * 8,
-                    "d2h_bytes_per_step": NS * N * 8, "seconds_per_step": round(e2e_s, 5)},
+            "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
         if sweep:
             line["sweep"] = sweep
+        if lob:
+            line["lobpcg"] = lob
         print(json.dumps(line), flush=True)
     H.close()
     ctx.close()
