@@ -157,6 +157,9 @@ typedef struct qg_lobpcg_options {
     int first_call;     /* 1: start with P = 0 and the 2n x 2n first step (reference is_first_time) */
     int precision;      /* QG_FP64: FP64 throughout */
     int verbose;        /* 1: print (iteration, max residual) lines to stdout */
+    int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
+                           applied in Fourier space with the FD stencil's own symbol */
+    double precond_shift; /* shift (Ha) of the kinetic preconditioner; <= 0 selects 1.0 */
 } qg_lobpcg_options;
 
 typedef struct qg_lobpcg_report {

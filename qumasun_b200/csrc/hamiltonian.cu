@@ -23,6 +23,7 @@
 
 #include "qg_internal.h"
 #include "stencil_common.cuh"
+#include "precond.h"
 
 namespace qg {
 
@@ -611,6 +612,7 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
 
 void destroy_ham(qg_hamiltonian h) {
     if (!h) return;
+    delete h->precond;
     cudaFree(h->V_d);
     cudaFree(h->V_f);
     free_projectors(h->pj);

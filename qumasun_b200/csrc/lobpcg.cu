@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "precond.h"
 #include "qg_internal.h"
 
 #define QG_BLAS_TRY(expr)                                                                   \
@@ -245,6 +246,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
     if (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0) return QG_ERR_INVALID;
     if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
+    if (opt->precond != 0 && opt->precond != 1) return QG_ERR_INVALID;
     const long long N = h->N();
     if ((long long)n * 3 > N) return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
@@ -285,7 +287,14 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     else QG_TRY(s.applyH(s.p, s.Ap));
     s.coldot(s.x, s.Ax, s.dV, s.ev_d);
     k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
-    {
+    qg::KineticPrecond* pc = nullptr;
+    if (opt->precond == 1) {
+        if (!h->precond) h->precond = new qg::KineticPrecond();
+        pc = h->precond;
+        QG_TRY(pc->setup(h, n, opt->precond_shift > 0 ? opt->precond_shift : 1.0));
+        QG_TRY(pc->apply(s.r, st));
+        s.normalize(s.r, nullptr);
+    } else {
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, 1.0, n, s.f_d);
         dim3 g((unsigned)std::min<long long>((N + 255) / 256, 64), n);
         k_scale_cols<<<g, 256, 0, st>>>(s.r, nullptr, N, N, s.f_d);
@@ -326,6 +335,10 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
         k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
         QG_CUDA_TRY(cudaGetLastError());
         QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (pc) {  // next search direction w = T r, normalised (the residual norms are already taken)
+            QG_TRY(pc->apply(s.r, st));
+            s.normalize(s.r, nullptr);
+        }
         QG_CUDA_TRY(cudaMemcpyAsync(&info_h, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
         tm.mark(5, st);
         tm.mark(-1, st);

@@ -75,6 +75,10 @@ struct DevProjectors {
     float* ent_val_f = nullptr;
 };
 
+namespace qg {
+struct KineticPrecond;
+}
+
 struct qg_hamiltonian_s {
     qg_context ctx = nullptr;
     int nx = 0, ny = 0, nz = 0;
@@ -88,6 +92,7 @@ struct qg_hamiltonian_s {
     DevBuf xio, hxio; // staging for the host-buffer entry point
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
+    qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
     long long N() const { return (long long)nx * ny * nz; }
 };
 

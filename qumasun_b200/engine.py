@@ -64,7 +64,8 @@ class LobpcgOptions(C.Structure):
     """qg_lobpcg_options."""
 
     _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("first_call", C.c_int),
-                ("precision", C.c_int), ("verbose", C.c_int)]
+                ("precision", C.c_int), ("verbose", C.c_int), ("precond", C.c_int),
+                ("precond_shift", C.c_double)]
 
 
 class LobpcgReport(C.Structure):
@@ -231,14 +232,15 @@ class Hamiltonian:
               "qg_hamiltonian_apply_noalloc_d")
         return out
 
-    def lobpcg(self, X0, max_iter=2000, tol=1.0e-10, P0=None, first=True, verbose=False):
+    def lobpcg(self, X0, max_iter=2000, tol=1.0e-10, P0=None, first=True, verbose=False, precond=0,
+               shift=1.0):
         """Block LOBPCG (qg_lobpcg_d) from host states X0 (ns, N); returns
         dict(ev, X, P, report, status). NOT_CONVERGED is reported, not raised."""
         X = np.ascontiguousarray(X0, dtype=np.float64).copy()
         ns = X.shape[0]
         P = np.zeros_like(X) if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).copy()
         ev = np.zeros(ns)
-        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0, precond, shift)
         rep = LobpcgReport()
         st = lib().qg_lobpcg_d(self.h, C.byref(opt), ns, ev.ctypes.data_as(_dp), X.ctypes.data, P.ctypes.data,
                                C.byref(rep))
