@@ -168,6 +168,8 @@ typedef struct qg_lobpcg_report {
     double max_residual;/* max_j sum_i r_j(i)^2 dV at exit */
     double ms_total;    /* device time of the solve */
     double ms_hamiltonian, ms_gram, ms_eigensolve, ms_rotate, ms_vector;  /* per-phase device time */
+    int restarts;       /* iterations whose [x r p] Gram matrix was singular and that
+                           continued from [x r] alone (P dropped) */
 } qg_lobpcg_report;
 
 /* Block LOBPCG for the ns lowest eigenpairs of H, FP64 on the GPU.
@@ -179,7 +181,11 @@ typedef struct qg_lobpcg_report {
  * DGEMMs (the w_dgemm path of lobpcg_d_multi_mpi.h:191-579) and the small
  * generalised eigenproblem solved on the GPU (replaces lapack_DSYGVX,
  * w_dsygvx.h:24-104). X (ns*N, in/out), P (ns*N, in/out, the reference's
- * "keep") and ev (ns, out) are HOST buffers, state-major. Returns
+ * "keep") and ev (ns, out) are HOST buffers, state-major. The pencil is
+ * Jacobi-equilibrated (scaled to unit diag(B)) and solved with cuSOLVER's
+ * sygvd; if B is still not positive definite the step continues from [x r]
+ * alone (P dropped, counted in report->restarts; pencils of up to 80 rows then
+ * go to the library's own one-block Jacobi solver). Returns
  * QG_ERR_NOT_CONVERGED (results still written) when max_iter is reached,
  * QG_ERR_CHOLESKY if the Gram matrix of [x r p] is not positive definite. */
 int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
@@ -187,6 +193,17 @@ int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double
 /* Same with DEVICE buffers X and P (ld = N); ev stays a host array. */
 int qg_lobpcg_d_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
                        double* X, double* P, qg_lobpcg_report* report);
+
+/* Batched small generalised eigensolver, FP64, DEVICE pointers, context stream:
+ * for b < batch, A_b z = lambda B_b z with A_b = A + b*stride, B_b = B + b*stride
+ * (k x k, column-major, leading dimension lda, lower triangles read), all k
+ * eigenpairs ascending into w + b*k and Z + b*k*k (column-major, ld k).
+ * Replaces lapack_DSYGVX (w_dsygvx.h:24-104: ITYPE 1, JOBZ V, RANGE A) for
+ * k <= 80; larger k returns QG_ERR_UNSUPPORTED. info (host, batch ints, may be
+ * NULL) receives 0, or 1 where B_b is not positive definite; the call waits
+ * for the stream when info is given. */
+int qg_sygv_small_batched_d(qg_context ctx, int batch, int k, const double* A, const double* B, int lda,
+                            long long stride, double* w, double* Z, int* info);
 
 /* Selects the stencil kernel of an operator: 0 = the TMA-staged ring kernel
  * where the shape and alignment allow (default), 1 = always the

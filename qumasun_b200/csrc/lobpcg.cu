@@ -8,8 +8,9 @@
 // One iteration:
 //   Ar = H r                                       (qg::apply_hamiltonian)
 //   Sa = W^T AW dV, Sb = W^T W dV                  (DGEMM; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
-//   Sa z = lambda Sb z, k = 3n (2n on the first step of a first call)   (cusolverDnDsygvd;
-//                                                   replaces DSYGVX, w_dsygvx.h:24-104, UPLO as the reference)
+//   Sa z = lambda Sb z, k = 3n (2n on the first step of a first call), Jacobi-equilibrated,
+//   cusolverDnDsygvd (replaces DSYGVX, w_dsygvx.h:24-104, UPLO as the reference); a
+//   singular [x r p] Gram matrix restarts the step from [x r] (P coefficients zero)
 //   p_new = [r p] [Cr; Cp], x_new = [x r p] [Cx; Cr; Cp] (DGEMM; lobpcg_d_multi.h:247-300)
 //   renormalise x, Ax by |x|, p, Ap by |p| (:491-505); ei = x.Ax dV; r = Ax - ei x (:506-512)
 //   stop when max_j sum r_j^2 dV < tol dV (:525).
@@ -25,6 +26,7 @@
 
 #include "precond.h"
 #include "qg_internal.h"
+#include "small_eig.h"
 
 #define QG_BLAS_TRY(expr)                                                                   \
     do {                                                                                    \
@@ -136,6 +138,30 @@ __global__ void __launch_bounds__(kRedThreads) k_residual(const double* __restri
     if (threadIdx.x == 0) nr[blockIdx.x] = s * dV;
 }
 
+// A2 = D A D, B2 = D B D on the leading k x k block (column-major, ld), D = diag(B)^-1/2;
+// one block per column
+__global__ void k_equilibrate(const double* __restrict__ A, const double* __restrict__ B, int ld, int k,
+                              double* __restrict__ A2, double* __restrict__ B2) {
+    const int j = blockIdx.x;
+    const double bj = B[j + (long long)j * ld];
+    const double dj = bj > 0.0 ? 1.0 / sqrt(bj) : 1.0;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const double bi = B[i + (long long)i * ld];
+        const double s = (bi > 0.0 ? 1.0 / sqrt(bi) : 1.0) * dj;
+        A2[i + (long long)j * ld] = A[i + (long long)j * ld] * s;
+        B2[i + (long long)j * ld] = B[i + (long long)j * ld] * s;
+    }
+}
+
+// Z(i, j) *= diag(B)(i)^-1/2 for rows i < k of the first gridDim.x columns
+__global__ void k_rowscale(double* __restrict__ Z, int ld, int k, const double* __restrict__ B, int ldb) {
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const double bi = B[i + (long long)i * ldb];
+        Z[i + (long long)j * ld] *= bi > 0.0 ? 1.0 / sqrt(bi) : 1.0;
+    }
+}
+
 struct Timer {
     cudaEvent_t ev[8];
     int n = 0;
@@ -175,7 +201,7 @@ struct Solver {
     cusolverDnHandle_t sol;
     DevBuf W, AW, T, AT, S, small, work;
     int lwork = 0;
-    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb;
+    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb, *Sa2, *Sb2;
     double *ev_d, *nr_d, *f_d, *f2_d, *w_d;
     int* info_d;
 
@@ -190,13 +216,13 @@ struct Solver {
         QG_TRY(T.reserve(2 * blk * sizeof(double)));
         QG_TRY(AT.reserve(2 * blk * sizeof(double)));
         const size_t k3 = 3 * (size_t)n;
-        QG_TRY(S.reserve(2 * k3 * k3 * sizeof(double)));
+        QG_TRY(S.reserve(4 * k3 * k3 * sizeof(double)));
         QG_TRY(small.reserve((5 * k3 + 16) * sizeof(double)));
         x = W.as<double>(); r = x + blk; p = r + blk;
         Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
         Tx = T.as<double>(); Tp = Tx + blk;
         ATx = AT.as<double>(); ATp = ATx + blk;
-        Sa = S.as<double>(); Sb = Sa + k3 * k3;
+        Sa = S.as<double>(); Sb = Sa + k3 * k3; Sa2 = Sb + k3 * k3; Sb2 = Sa2 + k3 * k3;
         ev_d = small.as<double>(); nr_d = ev_d + k3; f_d = nr_d + k3; f2_d = f_d + k3; w_d = f2_d + k3;
         info_d = reinterpret_cast<int*>(w_d + k3);
         QG_SOLVER_TRY(cusolverDnDsygvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
@@ -302,11 +328,11 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     QG_CUDA_TRY(cudaGetLastError());
 
     std::vector<double> ev_h(n), nr_h(n);
-    int info_h = 0;
     int it = 0;
     bool converged = false;
     double maxres = 0.0;
     int status = QG_OK;
+    int restarts = 0;
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
@@ -316,14 +342,52 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
         QG_TRY(s.gemm_tn(k3, k3, s.x, s.Ax, s.dV, s.Sa, k3));
         QG_TRY(s.gemm_tn(k3, k3, s.x, s.x, s.dV, s.Sb, k3));
         tm.mark(2, st);
-        QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
-                                       k3, s.Sa, k3, s.Sb, k3, s.w_d, s.work.as<double>(), s.lwork, s.info_d));
+        // Jacobi-equilibrated copy of the pencil (keeps the tiny residual columns of the
+        // reference iteration from ruining the Cholesky factor of B), cuSOLVER sygvd on it;
+        // if B is still not positive definite, restart this step without P
+        double* Z = s.Sa2;
+        bool restarted = false;
+        int solve_info = 0;
+        k_equilibrate<<<k3, 128, 0, st>>>(s.Sa, s.Sb, k3, k3, s.Sa2, s.Sb2);
+        QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k3,
+                                       s.Sa2, k3, s.Sb2, k3, s.w_d, s.work.as<double>(), s.lwork, s.info_d));
+        QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        if (solve_info > 0 && k3 == 3 * n) {
+            restarted = true;
+            if (k3 <= qg::kSmallEigMax) {
+                QG_TRY(qg::small_eig_launch(s.Sa, s.Sb, k3, 0, k3, 2 * n, Z, k3, 0, s.w_d, 0, s.info_d, 1, st));
+                QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+                QG_CUDA_TRY(cudaStreamSynchronize(st));
+                solve_info = (solve_info == 1) ? 1 : 0;  // the one-block solver returns scaled vectors
+            } else {
+                k_equilibrate<<<2 * n, 128, 0, st>>>(s.Sa, s.Sb, k3, 2 * n, s.Sa2, s.Sb2);
+                QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                               CUBLAS_FILL_MODE_LOWER, 2 * n, s.Sa2, k3, s.Sb2, k3, s.w_d,
+                                               s.work.as<double>(), s.lwork, s.info_d));
+                QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+                QG_CUDA_TRY(cudaStreamSynchronize(st));
+                if (solve_info == 0) {
+                    k_rowscale<<<n, 128, 0, st>>>(Z, k3, 2 * n, s.Sb, k3);
+                    QG_CUDA_TRY(cudaMemset2DAsync(Z + 2 * n, (size_t)k3 * sizeof(double), 0,
+                                                  (size_t)n * sizeof(double), (size_t)n, st));
+                }
+            }
+        } else if (solve_info == 0) {
+            k_rowscale<<<n, 128, 0, st>>>(Z, k3, k3, s.Sb, k3);  // z = D z'
+        }
+        if (solve_info != 0) {
+            status = solve_info > 0 ? QG_ERR_CHOLESKY : QG_ERR_LIBRARY;
+            ++it;
+            break;
+        }
+        if (restarted) ++restarts;
         tm.mark(3, st);
-        // rotation: columns 0..n-1 of Sa are (Cx; Cr; Cp)
-        QG_TRY(s.gemm_nn(k3 - n, s.r, s.Sa + n, k3, s.Tp));    // p_new = [r p] [Cr; Cp]
-        QG_TRY(s.gemm_nn(k3 - n, s.Ar, s.Sa + n, k3, s.ATp));
-        QG_TRY(s.gemm_nn(k3, s.x, s.Sa, k3, s.Tx));            // x_new = [x r p] [Cx; Cr; Cp]
-        QG_TRY(s.gemm_nn(k3, s.Ax, s.Sa, k3, s.ATx));
+        // rotation: columns 0..n-1 of Z are (Cx; Cr; Cp)
+        QG_TRY(s.gemm_nn(k3 - n, s.r, Z + n, k3, s.Tp));    // p_new = [r p] [Cr; Cp]
+        QG_TRY(s.gemm_nn(k3 - n, s.Ar, Z + n, k3, s.ATp));
+        QG_TRY(s.gemm_nn(k3, s.x, Z, k3, s.Tx));            // x_new = [x r p] [Cx; Cr; Cp]
+        QG_TRY(s.gemm_nn(k3, s.Ax, Z, k3, s.ATx));
         QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Ax, s.ATx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
@@ -339,16 +403,10 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
             QG_TRY(pc->apply(s.r, st));
             s.normalize(s.r, nullptr);
         }
-        QG_CUDA_TRY(cudaMemcpyAsync(&info_h, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
         tm.mark(5, st);
         tm.mark(-1, st);
         QG_CUDA_TRY(cudaStreamSynchronize(st));
         tm.flush();
-        if (info_h != 0) {
-            status = info_h > 0 ? QG_ERR_CHOLESKY : QG_ERR_LIBRARY;
-            ++it;
-            break;
-        }
         maxres = *std::max_element(nr_h.begin(), nr_h.end());
         if (!std::isfinite(maxres)) {
             status = QG_ERR_NONFINITE;
@@ -385,6 +443,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
         rep->ms_eigensolve = tm.acc[2];
         rep->ms_rotate = tm.acc[3];
         rep->ms_vector = tm.acc[4];
+        rep->restarts = restarts;
     }
     const int dstat = qg_context_take_device_status(h->ctx);
     if (dstat != QG_OK) return dstat;

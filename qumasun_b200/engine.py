@@ -73,7 +73,8 @@ class LobpcgReport(C.Structure):
 
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("max_residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_hamiltonian", C.c_double), ("ms_gram", C.c_double),
-                ("ms_eigensolve", C.c_double), ("ms_rotate", C.c_double), ("ms_vector", C.c_double)]
+                ("ms_eigensolve", C.c_double), ("ms_rotate", C.c_double), ("ms_vector", C.c_double),
+                ("restarts", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -111,6 +112,7 @@ def lib():
         L.qg_context_take_device_status.argtypes = [vp]
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
+        L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_lobpcg_d_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
@@ -164,6 +166,23 @@ class Context:
 
 def _ptr(a, t):
     return a.ctypes.data_as(t)
+
+
+def sygv_small_batched(ctx, A, B):
+    """Batched A z = lambda B z for torch CUDA float64 tensors (batch, k, k) (symmetric;
+    lower triangles read). Returns (w (batch, k), Z (batch, k, k) columns = eigenvectors, info)."""
+    import torch
+    bsz, k, _ = A.shape
+    At = A.transpose(1, 2).contiguous()   # column-major per problem
+    Bt = B.transpose(1, 2).contiguous()
+    w = torch.empty(bsz, k, dtype=torch.float64, device=A.device)
+    Z = torch.empty(bsz, k, k, dtype=torch.float64, device=A.device)
+    info = np.zeros(bsz, dtype=np.int32)
+    ctx.use_torch_stream()
+    check(lib().qg_sygv_small_batched_d(ctx.h, bsz, k, C.c_void_p(At.data_ptr()), C.c_void_p(Bt.data_ptr()), k,
+                                        k * k, C.c_void_p(w.data_ptr()), C.c_void_p(Z.data_ptr()),
+                                        info.ctypes.data_as(_ip)), "qg_sygv_small_batched_d")
+    return w, Z.transpose(1, 2), info
 
 
 class Hamiltonian:
