@@ -98,6 +98,8 @@ def port_lib():
         lib.or_hamiltonian_apply.argtypes = [C.POINTER(HamDescC), C.c_int, _dp, _dp]
         lib.or_hamiltonian_kpoint_local.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
                                                     C.c_double, C.c_int, _dp, _dp]
+        lib.or_hamiltonian_kpoint_apply.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
+                                                    C.c_double, C.c_int, _dp, _dp]
         _port = lib
     return _port
 
@@ -122,6 +124,8 @@ def ref_lib():
                                            C.c_int, C.c_int, _ip]
         lib.ref_grid_for_sphere.argtypes = [C.c_double] * 7 + [_ip]
         lib.ref_ylm_cube.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp]
+        lib.ref_hamiltonian_kpoint_apply.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
+                                                     C.c_double, C.c_double, C.c_int, _dp, _dp]
         _ref = lib
     return _ref
 
@@ -178,6 +182,23 @@ def hamiltonian_kpoint_local(cell, g, X):
     desc = HamDesc(cell, 8)
     port_lib().or_hamiltonian_kpoint_local(C.byref(desc.c), g[0], g[1], g[2], X.shape[0],
                                            _ptr(X, _dp), _ptr(HX, _dp))
+    return HX
+
+
+def hamiltonian_kpoint_apply(cell, g, X, impl="port"):
+    """Complex k-point H (V + nonlocal with Bloch phases + 8th-order k-point kinetic)
+    on {re, im} states X (ns, 2N); g = Bloch vector in bohr^-1."""
+    X = _c64(X)
+    HX = np.zeros_like(X)
+    desc = HamDesc(cell, 8)
+    if impl == "port":
+        rc = port_lib().or_hamiltonian_kpoint_apply(C.byref(desc.c), g[0], g[1], g[2], X.shape[0],
+                                                    _ptr(X, _dp), _ptr(HX, _dp))
+    else:
+        rc = ref_lib().ref_hamiltonian_kpoint_apply(C.byref(desc.c), g[0], g[1], g[2], cell.cutoff,
+                                                    X.shape[0], _ptr(X, _dp), _ptr(HX, _dp))
+    if rc != 0:
+        raise ValueError(f"hamiltonian_kpoint_apply rejected ({rc})")
     return HX
 
 

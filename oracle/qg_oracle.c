@@ -250,3 +250,75 @@ int or_hamiltonian_kpoint_local(const or_ham_desc* d, double gx, double gy, doub
     }
     return 0;
 }
+
+/* ProjectionPP of PseudoPotIntegrator_kpoint (PseudoPotOperator_kpoint_v2.h:2581-2700)
+ * for one {re, im} state. The projector on cube point q of atom a is
+ *   P(q) = w_k(q) Y(q) exp(i theta(q)),  theta = gx hx ux + gy hy uy + gz hz uz,
+ * u the point's unwrapped grid coordinate (mCreateProjectorRadialOnBlock, :287-420).
+ * Contraction without conjugate (mInnerNonlocalPsi_v2, :836-905):
+ *   c = dV (Y00 for l = 0) sum_q P(q) psi(g(q));
+ * scatter with the conjugate: Hpsi(g(q)) += E (Y00 for l = 0) conj(P(q)) c. */
+static void nonlocal_kpoint_one(const or_ham_desc* d, double gx, double gy, double gz, const double* re,
+                                const double* im, double* ore, double* oim) {
+    const double dV = d->hx * d->hy * d->hz;
+    const double Y00 = 1.0 / sqrt(4.0 * M_PI);
+    const int nx = d->nx, ny = d->ny, nz = d->nz;
+    const double ax = gx * d->hx, ay = gy * d->hy, az = gz * d->hz;
+    for (int a = 0; a < d->n_atoms; ++a) {
+        for (int k = 0; k < d->n_proj; ++k) {
+            const int l = d->proj_l[k];
+            const int* c = d->cube + 6 * ((size_t)a * d->n_proj + k);
+            const int bx = c[0], by = c[1], bz = c[2], sx = c[3], sy = c[4], sz = c[5];
+            const double* w = d->w_data + d->w_off[(size_t)a * d->n_proj + k];
+            const int nm = 2 * l + 1;
+            for (int m1 = 0; m1 < nm; ++m1) {
+                const double* Y = (l == 0) ? NULL : d->ylm_data + d->ylm_off[(size_t)a * d->n_lm + l * l + m1];
+                double sr = 0.0, si = 0.0;
+                for (int kz = 0; kz < sz; ++kz)
+                    for (int ky = 0; ky < sy; ++ky)
+                        for (int kx = 0; kx < sx; ++kx) {
+                            const size_t q = kx + (size_t)sx * (ky + (size_t)sy * kz);
+                            const double th = ax * (double)(bx + kx) + ay * (double)(by + ky) + az * (double)(bz + kz);
+                            const double p = Y ? w[q] * Y[q] : w[q];
+                            const double pr = p * cos(th), pi = p * sin(th);
+                            const size_t g = (size_t)wrapi(bx + kx, nx) +
+                                             (size_t)nx * ((size_t)wrapi(by + ky, ny) + (size_t)ny * (size_t)wrapi(bz + kz, nz));
+                            sr += pr * re[g] - pi * im[g];
+                            si += pi * re[g] + pr * im[g];
+                        }
+                const double s = (l == 0) ? dV * Y00 * Y00 * d->proj_E[k] : dV * d->proj_E[k];
+                const double cr = sr * s, ci = si * s;
+                for (int kz = 0; kz < sz; ++kz)
+                    for (int ky = 0; ky < sy; ++ky)
+                        for (int kx = 0; kx < sx; ++kx) {
+                            const size_t q = kx + (size_t)sx * (ky + (size_t)sy * kz);
+                            const double th = ax * (double)(bx + kx) + ay * (double)(by + ky) + az * (double)(bz + kz);
+                            const double p = Y ? w[q] * Y[q] : w[q];
+                            const double pr = p * cos(th), pi = p * sin(th);
+                            const size_t g = (size_t)wrapi(bx + kx, nx) +
+                                             (size_t)nx * ((size_t)wrapi(by + ky, ny) + (size_t)ny * (size_t)wrapi(bz + kz, nz));
+                            ore[g] += pr * cr + pi * ci;
+                            oim[g] += pr * ci - pi * cr;
+                        }
+            }
+        }
+    }
+}
+
+/* Complex k-point Hamiltonian, mHamiltonianMatrix_ddm of QUMASUN_KPOINT
+ * (qumasun_kpoint.matrix.h:25-50): V on re and im, the k-point nonlocal term,
+ * then the 8th-order k-point kinetic term. Each state is {re[N], im[N]} contiguous. */
+int or_hamiltonian_kpoint_apply(const or_ham_desc* d, double gx, double gy, double gz, int ns, const double* X,
+                                double* HX) {
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    for (int s = 0; s < ns; ++s) {
+        const double* re = X + (size_t)s * 2 * N;
+        const double* im = re + N;
+        double* ore = HX + (size_t)s * 2 * N;
+        double* oim = ore + N;
+        for (size_t i = 0; i < N; ++i) { ore[i] = d->V[i] * re[i]; oim[i] = d->V[i] * im[i]; }
+        if (d->n_atoms > 0 && d->n_proj > 0) nonlocal_kpoint_one(d, gx, gy, gz, re, im, ore, oim);
+        or_laplacian_kpoint8(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, gx, gy, gz, re, im, ore, oim);
+    }
+    return 0;
+}

@@ -18,6 +18,11 @@
  *   ref_lobpcg_d_multi     -> EigenLOBPCG_d_multi (lobpcg_d_multi.h:23-545)
  *   ref_grid_for_sphere    -> GridForSphere (GridSubgrid.h:482-492)
  *   ref_ylm_cube           -> SetYlmAround<L,M> (PseudoPotOperator.h:58-71)
+ *   ref_hamiltonian_kpoint_apply
+ *                          -> mHamiltonianMatrix_ddm of QUMASUN_KPOINT (qumasun_kpoint.matrix.h:25-50):
+ *                             zero, V on re and im, PseudoPotIntegrator_kpoint::ProjectionPP
+ *                             (PseudoPotOperator_kpoint_v2.h:2581-2700, its Gamma branch included),
+ *                             LaplasianKpoint8th (coef -1/2)
  *
  * The projector tables are injected in the reference's own cube form
  * (PP_nonlocal_each_atom: one SubspaceField per projector w_k and per Y_lm),
@@ -60,6 +65,7 @@ inline int lapack_DSYGVX(double* A, double* B, double* ev, double* evec, double*
 #define private public
 #define protected public
 #include "PseudoPotOperator.h"
+#include "PseudoPotOperator_kpoint_v2.h"
 #undef private
 #undef protected
 
@@ -286,6 +292,167 @@ int ref_lobpcg_d_multi(const ref_ham_desc* d, int ns, int iter_max, double* ev, 
         EigenLOBPCG_d_multi(N, dV, ns, iter_max, ev, X, P, work.data(), is_first_time != 0, OpeA, watch);
     }
     if (iters) *iters = (int)((calls - 2LL * ns) / ns);
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+/* Owns a PseudoPotIntegrator_kpoint set up by the reference's own routines:
+ * per-l blocks from GridForSphere + GetOverlapPeriodic (the two calls of
+ * UpdatePositionLocal, PseudoPotOperator_vlocal.h:155-165), projector counts
+ * (CountNonlocalProjector, mSetNonlocalProjectorInfo), Y_lm on the blocks
+ * (tCreateProjectorYlmOnBlock) and the Bloch phases (UpdateNonlocalBlock ->
+ * mCreateProjectorRadialOnBlock[_gamma], PseudoPotOperator_kpoint_v2.h:287-420).
+ * The radial table handed to the reference is the constant 1 (every point lies
+ * inside radius[0], so the reference takes p = projector[2k][0] = 1 without
+ * interpolation); the harness then multiplies each block value by the
+ * analytic w_k of the matching cube point, so projector_expikx ends up as
+ * w_k(r) * exp(i g.r) with the reference's own phases and block layout. */
+struct RefKpointHamiltonian {
+    const ref_ham_desc* d;
+    double g[3];
+    PseudoPotIntegrator_kpoint pp;
+    std::vector<Nucleus> nuclei;
+    GridRangeMPI grid;
+    int status = 0;
+
+    RefKpointHamiltonian(const ref_ham_desc* desc, double gx, double gy, double gz, double rc) : d(desc) {
+        g[0] = gx; g[1] = gy; g[2] = gz;
+        std::memset(static_cast<void*>(&grid), 0, sizeof(grid));
+        grid.begin_x = 0; grid.begin_y = 0; grid.begin_z = 0;
+        grid.end_x = d->nx; grid.end_y = d->ny; grid.end_z = d->nz;
+        grid.mpi_comm = MPI_COMM_WORLD;
+        GridInfo gi;
+        gi.size_x = d->nx; gi.size_y = d->ny; gi.size_z = d->nz;
+        gi.size_3d = (size_t)d->nx * d->ny * d->nz;
+        pp.InitializeGrid(gi, d->hx, d->hy, d->hz);
+        const int Z = 6;
+        for (int a = 0; a < d->n_atoms; ++a)
+            nuclei.push_back(Nucleus{Z, d->atom_pos[3 * a], d->atom_pos[3 * a + 1], d->atom_pos[3 * a + 2]});
+        if (d->n_atoms <= 0 || d->n_proj <= 0) return;
+        const int np = d->n_proj;
+        PseudoPot_MBK* mbk = new PseudoPot_MBK();
+        mbk->num_projectors = np;
+        mbk->projector_quantum_l = new int[np];
+        mbk->projector_energy_up = new double[np];
+        for (int k = 0; k < np; ++k) {
+            mbk->projector_quantum_l[k] = d->proj_l[k];
+            mbk->projector_energy_up[k] = d->proj_E[k];
+        }
+        mbk->num_radial_grids = 2;
+        mbk->buffer_all = new double[2 + 4 * np];
+        mbk->radius = mbk->buffer_all;
+        mbk->radius[0] = 1.0e6;
+        mbk->radius[1] = 2.0e6;
+        for (int j = 0; j < 2 * np; ++j) {
+            double* pr = mbk->buffer_all + 2 + 2 * j;
+            pr[0] = 1.0;
+            pr[1] = 1.0;
+            mbk->projector.push_back(pr);
+        }
+        mbk->xi_min = 0.0;
+        mbk->xi_delta = 1.0;
+        for (int l = 0; l < 4; ++l) mbk->cutoff_r[l] = rc;
+        pp.m_pp_list.emplace(Z, mbk);
+
+        const int max_l = mbk->MaxProjectorL();
+        pp.m_nonlocal_blocks.resize(d->n_atoms);
+        size_t max_grid = 0;
+        for (int a = 0; a < d->n_atoms; ++a) {
+            auto& blocks = pp.m_nonlocal_blocks[a];
+            blocks.resize(max_l + 1);
+            for (int l = 0; l <= max_l; ++l) {
+                blocks[l].cutoff = rc;
+                GridRange sub = GridForSphere(nuclei[a].Rx, nuclei[a].Ry, nuclei[a].Rz, rc, d->hx, d->hy, d->hz);
+                /* the injected w cubes must sit on exactly this subgrid */
+                for (int k = 0; k < np; ++k) {
+                    if (d->proj_l[k] != l) continue;
+                    const int* c = d->cube + 6 * ((size_t)a * np + k);
+                    if (c[0] != sub.begin_x || c[1] != sub.begin_y || c[2] != sub.begin_z ||
+                        c[3] != sub.end_x - sub.begin_x || c[4] != sub.end_y - sub.begin_y ||
+                        c[5] != sub.end_z - sub.begin_z)
+                        status = -2;
+                }
+                blocks[l].grid_sizes = GetOverlapPeriodic(grid, sub, d->nx, d->ny, d->nz, blocks[l].range_blocks,
+                                                          blocks[l].shifted_grids);
+                max_grid = std::max(max_grid, (size_t)blocks[l].grid_sizes);
+            }
+        }
+        if (status) return;
+        pp.m_max_grid_size = max_grid;
+        pp.CountNonlocalProjector(nuclei.data(), d->n_atoms);
+        pp.m_nonlocal_projectors.clear();
+        pp.m_nonlocal_projectors.resize(d->n_atoms);
+        for (int a = 0; a < d->n_atoms; ++a) {
+            pp.mSetNonlocalProjectorInfo(pp.m_nonlocal_projectors[a], nuclei[a]);
+            tCreateProjectorYlmOnBlock(pp.m_nonlocal_blocks[a], pp.m_nonlocal_projectors[a], nuclei[a], d->hx, d->hy,
+                                       d->hz, grid);
+        }
+        pp.m_comm4atoms.comm_4_nuclei.assign(d->n_atoms, MPI_COMM_WORLD);
+        pp.m_request4atoms.resize(d->n_atoms);
+        pp.m_status4atoms.resize(d->n_atoms);
+        pp.UpdateNonlocalBlock(nuclei.data(), d->n_atoms, grid, 0, gx * d->hx, gy * d->hy, gz * d->hz);
+        /* w_k onto the blocks (same point order as mCreateProjectorRadialOnBlock) */
+        for (int a = 0; a < d->n_atoms; ++a) {
+            auto& proj = pp.m_nonlocal_projectors[a];
+            for (int k = 0; k < np; ++k) {
+                const int l = d->proj_l[k];
+                const auto& blk = pp.m_nonlocal_blocks[a][l];
+                const int* c = d->cube + 6 * ((size_t)a * np + k);
+                const double* w = d->w_data + d->w_off[(size_t)a * np + k];
+                SoAComplex& pb = proj.projector_expikx[0][k];
+                int off = 0;
+                for (size_t ib = 0; ib < blk.range_blocks.size(); ++ib) {
+                    const GridRange& r = blk.range_blocks[ib];
+                    const auto& sh = blk.shifted_grids[ib];
+                    const int sx = r.end_x - r.begin_x, sy = r.end_y - r.begin_y;
+                    for (int iz = r.begin_z; iz < r.end_z; ++iz)
+                        for (int iy = r.begin_y; iy < r.end_y; ++iy)
+                            for (int ix = r.begin_x; ix < r.end_x; ++ix) {
+                                const int i = off + (ix - r.begin_x) + sx * ((iy - r.begin_y) + sy * (iz - r.begin_z));
+                                const int qx = ix - sh.x - c[0], qy = iy - sh.y - c[1], qz = iz - sh.z - c[2];
+                                const double wv = w[qx + (size_t)c[3] * (qy + (size_t)c[4] * qz)];
+                                pb.re[i] *= wv;
+                                if (pb.im) pb.im[i] *= wv;
+                            }
+                    off += r.Size3D();
+                }
+            }
+        }
+    }
+
+    /* One {re, im} state, in the order of mHamiltonianMatrix_ddm (qumasun_kpoint.matrix.h:25-50). */
+    void Apply(double* ore, double* oim, const double* re, const double* im) {
+        const size_t N = (size_t)d->nx * d->ny * d->nz;
+        for (size_t i = 0; i < N; ++i) { ore[i] = 0.0; oim[i] = 0.0; }
+        for (size_t i = 0; i < N; ++i) ore[i] = d->V[i] * re[i];
+        for (size_t i = 0; i < N; ++i) oim[i] = d->V[i] * im[i];
+        if (d->n_atoms > 0 && d->n_proj > 0) {
+            SoAComplex hp{ore, oim};
+            SoAComplex ps{const_cast<double*>(re), const_cast<double*>(im)};
+            pp.ProjectionPP(hp, ps, grid, nuclei.data(), d->n_atoms, 0);
+        }
+        ref_laplacian_kpoint8(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, g[0], g[1], g[2], re, im, ore, oim);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+/* HX[s] = H_k X[s] for ns complex states, each {re[N], im[N]} contiguous (X[s*2N + i],
+ * X[s*2N + N + i]); g = Bloch vector (bohr^-1); rc = projector cutoff radius that made
+ * the cubes in d. Returns -2 if a cube differs from GridForSphere(R, rc). */
+int ref_hamiltonian_kpoint_apply(const ref_ham_desc* d, double gx, double gy, double gz, double rc, int ns,
+                                 const double* X, double* HX) {
+    if (d->fd_order != 8) return -1;
+    RefKpointHamiltonian H(d, gx, gy, gz, rc);
+    if (H.status) return H.status;
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    for (int s = 0; s < ns; ++s)
+        H.Apply(HX + (size_t)s * 2 * N, HX + (size_t)s * 2 * N + N, X + (size_t)s * 2 * N, X + (size_t)s * 2 * N + N);
     return 0;
 }
 

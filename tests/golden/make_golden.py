@@ -4,7 +4,9 @@ Run where the reference tree exists and `make -C oracle` has built
 oracle/_ref/libqumasun_ref.so:  python tests/golden/make_golden.py
 Every array comes from the reference functions driven by oracle/ref_harness.cpp:
 Laplasian{2,4,6,8}th_halo, LaplasianKpoint8th_halo, the reference Hamiltonian
-(V, ProjectionPP, kinetic) and GridForSphere / SetYlmAround tables.
+(V, ProjectionPP, kinetic), the reference k-point Hamiltonian (V,
+PseudoPotIntegrator_kpoint::ProjectionPP, LaplasianKpoint8th; `--kpoint` writes
+only ham_kpoint.npz) and GridForSphere / SetYlmAround tables.
 """
 import os
 import sys
@@ -70,8 +72,48 @@ def main():
     print("wrote lobpcg_small", r["iters"], r["ev"])
 
 
-if __name__ == "__main__":
+def smooth_state(cell):
+    """{re, im} of one smooth state: Gaussians (width 1.2 bohr) centred on atoms 0 and 1."""
+    out = []
+    for a in (0, 1):
+        R = cell.positions[a]
+        x = cell.hx * np.arange(cell.nx) - R[0]
+        y = cell.hy * np.arange(cell.ny) - R[1]
+        z = cell.hz * np.arange(cell.nz) - R[2]
+        rr = z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2
+        out.append(np.exp(-rr / (2 * 1.2 ** 2)).reshape(-1))
+    return np.concatenate(out)
+
+
+# k-point cases: Gamma, a commensurate k (a quarter and a half of the cell's
+# reciprocal vectors) and a general k; "wrap" cubes exceed the cell, so one grid
+# point carries several periodic images of an atom with different Bloch phases.
+KPOINT_CASES = [
+    ("noncubic", dict(grid=(20, 16, 24), displacement=0.05, seed=3)),
+    ("wrap", dict(grid=(12, 12, 12), a0=4.4)),
+]
+
+
+def make_kpoint():
+    out = {}
+    for name, kw in KPOINT_CASES:
+        cell = build_cell(**kw)
+        X = np.stack([initial_states(1, 2 * cell.N, seed=13)[0], smooth_state(cell)])
+        L = np.array([cell.nx * cell.hx, cell.ny * cell.hy, cell.nz * cell.hz])
+        gs = [(0.0, 0.0, 0.0), tuple(2 * np.pi / L * np.array([0.25, -0.5, 0.25])), (0.31, -0.17, 0.05)]
+        out[f"{name}_X"] = X
+        out[f"{name}_g"] = np.array(gs)
+        for i, g in enumerate(gs):
+            out[f"{name}_HX{i}"] = O.hamiltonian_kpoint_apply(cell, g, X, impl="ref")
+    np.savez_compressed(os.path.join(HERE, "ham_kpoint.npz"), **out)
+    print("wrote ham_kpoint")
+
+
+if __name__ == "__main__" and "--kpoint" in sys.argv:
+    make_kpoint()
+elif __name__ == "__main__" and "--diamond8" not in sys.argv:
     main()
+    make_kpoint()
 
 # lobpcg_diamond8.npz (the 8-atom 40^3 cell, 16 states, seed 1234, FD order 8) is
 # the output of oracle.ref_lobpcg_d_multi(build_cell(), initial_states(16, 64000,

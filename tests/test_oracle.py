@@ -80,3 +80,76 @@ def test_port_matches_live_reference_on_fresh_cell():
     a = O.hamiltonian_apply(cell, X, impl="port")
     b = O.hamiltonian_apply(cell, X, impl="ref")
     assert max(rel(a[s], b[s]) for s in range(3)) < 1e-14
+
+
+# ---------------------------------------------------------------- k-point H
+KPOINT_CASES = {"noncubic": dict(grid=(20, 16, 24), displacement=0.05, seed=3),
+                "wrap": dict(grid=(12, 12, 12), a0=4.4)}
+
+
+@pytest.fixture(scope="module")
+def kpoint_gold():
+    return np.load(os.path.join(GOLD, "ham_kpoint.npz"))
+
+
+@pytest.mark.parametrize("name", sorted(KPOINT_CASES))
+def test_port_kpoint_hamiltonian_matches_reference(kpoint_gold, name):
+    # PseudoPotIntegrator_kpoint::ProjectionPP + LaplasianKpoint8th (qumasun_kpoint.matrix.h:25-50)
+    cell = build_cell(**KPOINT_CASES[name])
+    X = kpoint_gold[f"{name}_X"]
+    for i, g in enumerate(kpoint_gold[f"{name}_g"]):
+        ref = kpoint_gold[f"{name}_HX{i}"]
+        HX = O.hamiltonian_kpoint_apply(cell, tuple(g), X)
+        loc = O.hamiltonian_kpoint_local(cell, tuple(g), X)
+        for s in range(2):
+            assert rel(HX[s], ref[s]) < 1e-14
+            # the nonlocal part alone, relative to its own size (for the random state it is
+            # ~4e-4 of the total, so the subtraction costs about three digits)
+            assert rel(HX[s] - loc[s], ref[s] - loc[s]) < 1e-12
+
+
+def test_port_kpoint_nonlocal_is_gauge_covariant_for_commensurate_k():
+    # For g a reciprocal vector of the cell the Bloch phase is periodic on the
+    # grid, so V_NL(g) u = exp(-i g.r) V_NL(0) (exp(i g.r) u) holds exactly.
+    cell = build_cell(grid=(20, 16, 24), displacement=0.05, seed=3)
+    N = cell.N
+    L = np.array([cell.nx * cell.hx, cell.ny * cell.hy, cell.nz * cell.hz])
+    g = 2 * np.pi / L * np.array([1.0, -2.0, 1.0])
+    u = initial_states(1, 2 * N, seed=21)[0]
+    uc = u[:N] + 1j * u[N:]
+    ix = np.arange(cell.nx) * cell.hx
+    iy = np.arange(cell.ny) * cell.hy
+    iz = np.arange(cell.nz) * cell.hz
+    phase = np.exp(1j * (g[2] * iz[:, None, None] + g[1] * iy[None, :, None] + g[0] * ix[None, None, :])).reshape(-1)
+
+    def nl(gv, vec):
+        X = np.concatenate([vec.real, vec.imag])[None]
+        out = O.hamiltonian_kpoint_apply(cell, tuple(gv), X) - O.hamiltonian_kpoint_local(cell, tuple(gv), X)
+        return out[0, :N] + 1j * out[0, N:]
+
+    lhs = nl(g, uc)
+    rhs = np.conj(phase) * nl((0.0, 0.0, 0.0), phase * uc)
+    assert np.linalg.norm(lhs - rhs) / np.linalg.norm(lhs) < 1e-12
+
+
+def test_port_kpoint_hamiltonian_is_hermitian():
+    cell = build_cell(grid=(20, 16, 24), displacement=0.05, seed=3)
+    N = cell.N
+    g = (0.31, -0.17, 0.05)
+    X = initial_states(2, 2 * N, seed=17)
+    HX = O.hamiltonian_kpoint_apply(cell, g, X)
+    z = X[:, :N] + 1j * X[:, N:]
+    hz = HX[:, :N] + 1j * HX[:, N:]
+    a = np.vdot(z[0], hz[1])
+    b = np.conj(np.vdot(z[1], hz[0]))
+    assert abs(a - b) < 1e-12 * abs(a)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_port_kpoint_matches_live_reference_on_fresh_cell():
+    cell = build_cell(grid=(16, 20, 12), displacement=0.2, seed=4)
+    X = initial_states(2, 2 * cell.N, seed=98)
+    g = (-0.2, 0.45, 0.1)
+    a = O.hamiltonian_kpoint_apply(cell, g, X, impl="port")
+    b = O.hamiltonian_kpoint_apply(cell, g, X, impl="ref")
+    assert rel(a, b) < 1e-14
