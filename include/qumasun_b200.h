@@ -122,6 +122,26 @@ int qg_hamiltonian_apply_f(qg_hamiltonian ham, int ns, const float* X, long long
  * applies H, copies HX back, and returns after HX is on the host. */
 int qg_hamiltonian_apply_host_d(qg_hamiltonian ham, int ns, const double* X, double* HX);
 
+/* Complex k-point operator H_k u = V u + V_NL(g) u - 1/2 (Lap + 2i g.grad - g^2) u
+ * for ns split-complex states, DEVICE pointers, FP64: state s has its real part
+ * at X + s*ldx and its imaginary part at X + s*ldx + N (ldx, ldhx >= 2N), the
+ * reference's {re[N], im[N]} state layout (lobpcg_z_multi_mpi.h:1005-1012).
+ * g is the operator's Bloch vector (descriptor or qg_hamiltonian_set_kvector);
+ * the projectors carry exp(i g.r) at the unwrapped image position of each
+ * cube point. FD order 8 only (KINETIC_8TH; other orders QG_ERR_UNSUPPORTED).
+ * Replaces OpeA(SoAComplex& Ax, const SoAComplex& x) of qumasun_kpoint.lobpcg.h:38-40
+ * -> QUMASUN_KPOINT::mHamiltonianMatrix_ddm (qumasun_kpoint.matrix.h:25-50):
+ * mPotentialMatrix_ddm on re and im, PseudoPotIntegrator_kpoint::ProjectionPP
+ * (PseudoPotOperator_kpoint_v2.h:2581-2700), LaplasianKpoint8th_ddm
+ * (GridDifferenceKpoint8th.h:325-368). */
+int qg_hamiltonian_apply_z(qg_hamiltonian ham, int ns, const double* X, long long ldx,
+                           double* HX, long long ldhx);
+/* qg_hamiltonian_apply_z with HOST buffers (ns * 2N doubles each, ldx = 2N). */
+int qg_hamiltonian_apply_host_z(qg_hamiltonian ham, int ns, const double* X, double* HX);
+/* qg_hamiltonian_apply_z with the phase timing of qg_hamiltonian_apply_timed_d. */
+int qg_hamiltonian_apply_timed_z(qg_hamiltonian ham, int ns, const double* X, long long ldx,
+                                 double* HX, long long ldhx, float* ms_phases);
+
 /* qg_hamiltonian_apply_d with device-side phase timing (CUDA events on the
  * context stream; the call synchronizes): ms_phases[0] = projector
  * gather-contraction, [1] = stencil + local potential, [2] = nonlocal scatter

@@ -500,7 +500,7 @@ int upload(T** dst, const std::vector<T>& src) {
 void free_projectors(DevProjectors& pj) {
     cudaFree(pj.atom_off); cudaFree(pj.pt_g); cudaFree(pj.tab_d); cudaFree(pj.tab_f);
     cudaFree(pj.ch_scale); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
-    cudaFree(pj.ent_val_f);
+    cudaFree(pj.ent_val_f); cudaFree(pj.pt_u); cudaFree(pj.ent_pt); cudaFree(pj.ztab); cudaFree(pj.zent);
     pj = DevProjectors{};
 }
 
@@ -524,7 +524,7 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
     const long long N = h->N();
 
     std::vector<int> atom_off(na + 1, 0);
-    std::vector<int> pt_g;
+    std::vector<int> pt_g, pt_u;
     std::vector<std::vector<double>> tabs(nch);
     std::vector<double> ch_scale((size_t)na * nch, 0.0);
     std::vector<int> ch_k(nch, -1), ch_m(nch, 0);
@@ -572,6 +572,7 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
                     if (!any) continue;
                     const long long g = wrap_host(x, nx) + (long long)nx * (wrap_host(y, ny) + (long long)ny * wrap_host(z, nz));
                     pt_g.push_back((int)g);
+                    pt_u.push_back(x); pt_u.push_back(y); pt_u.push_back(z);
                     for (int ch = 0; ch < nch; ++ch) tabs[ch].push_back(vals[ch]);
                 }
         atom_off[a + 1] = (int)pt_g.size();
@@ -586,12 +587,13 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
     for (long long p = 0; p < npts; ++p) row[pt_g[p] + 1]++;
     for (long long g = 0; g < N; ++g) row[g + 1] += row[g];
     std::vector<int> fill(row.begin(), row.end() - 1);
-    std::vector<int> ent_atom(npts);
+    std::vector<int> ent_atom(npts), ent_pt(npts);
     std::vector<double> ent_val((size_t)npts * nch);
     for (int a = 0; a < na; ++a)
         for (int p = atom_off[a]; p < atom_off[a + 1]; ++p) {
             const int e = fill[pt_g[p]]++;
             ent_atom[e] = a;
+            ent_pt[e] = p;
             for (int ch = 0; ch < nch; ++ch) ent_val[(size_t)e * nch + ch] = tab_d[(size_t)ch * npts + p];
         }
     std::vector<float> ent_val_f(ent_val.begin(), ent_val.end());
@@ -607,6 +609,8 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
     QG_TRY(upload(&pj.ent_atom, ent_atom));
     QG_TRY(upload(&pj.ent_val_d, ent_val));
     QG_TRY(upload(&pj.ent_val_f, ent_val_f));
+    QG_TRY(upload(&pj.pt_u, pt_u));
+    QG_TRY(upload(&pj.ent_pt, ent_pt));
     return QG_OK;
 }
 

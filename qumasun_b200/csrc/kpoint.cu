@@ -1,0 +1,373 @@
+// Complex k-point Hamiltonian on the device (mHamiltonianMatrix_ddm of
+// QUMASUN_KPOINT, qumasun_kpoint.matrix.h:25-50):
+//   H_k u = V u + sum_atoms sum_k E_k sum_m conj(P_km) dV (P_km . u) - 1/2 (Lap + 2i g.grad - g^2) u,
+//   P_km(r) = w_k(r) Y_lm(r) exp(i g.r) at the unwrapped image position of each cube point
+//   (mCreateProjectorRadialOnBlock, PseudoPotOperator_kpoint_v2.h:287-420; ProjectionPP :2581-2700).
+// States are split complex, one state = {re[N], im[N]} (lobpcg_z_multi_mpi.h:1005-1012).
+// Three launches for a block of states, as on the real path:
+//   k_project_z     c[s][a,ch] = E dV sum_p P(p) u_s(g(p))          (no conjugate, mInnerNonlocalPsi_v2)
+//   k_stencil_tma   V u - 1/2 (Lap + 2i g.grad - g^2) u, both parts of a plane staged together
+//                   (stencil_tma.cu, NC = 2); any other shape runs k_kpoint_plain
+//   k_scatter_all_z Hu[s][g] += sum_entries conj(P) c                 (the scatter of ProjectionPP)
+// The Bloch-phase tables are rebuilt on the device by k_bloch_tables whenever
+// the k-vector differs from the one they were built for.
+#include <algorithm>
+#include <cmath>
+
+#include "qg_internal.h"
+#include "stencil_common.cuh"
+
+namespace qg {
+namespace {
+
+// ztab / zent for the k-vector g (see DevProjectors). theta = (ax ux + ay uy) + az uz,
+// a* = g* h*, as the reference sums kxx + kyy + kzz.
+__global__ void k_bloch_tables(const double* __restrict__ tab, const int* __restrict__ pt_u, long long npts,
+                               const int* __restrict__ ent_pt, long long nent, int nch, double ax, double ay,
+                               double az, double* __restrict__ ztab, double* __restrict__ zent) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npts + nent; i += stride) {
+        const long long p = i < npts ? i : ent_pt[i - npts];
+        const double th = __dadd_rn(__dadd_rn(__dmul_rn(ax, (double)pt_u[3 * p]), __dmul_rn(ay, (double)pt_u[3 * p + 1])),
+                                    __dmul_rn(az, (double)pt_u[3 * p + 2]));
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        if (i < npts) {
+            for (int c = 0; c < nch; ++c) {
+                const double v = tab[(long long)c * npts + p];
+                ztab[(long long)c * npts + p] = v * cs;
+                ztab[(long long)(nch + c) * npts + p] = v * sn;
+            }
+        } else {
+            const long long e = i - npts;
+            for (int c = 0; c < nch; ++c) {
+                const double v = tab[(long long)c * npts + p];
+                zent[(e * nch + c) * 2] = v * cs;
+                zent[(e * nch + c) * 2 + 1] = v * sn;
+            }
+        }
+    }
+}
+
+// Complex gather-contraction: one block per (atom, group of SB states).
+// c = sum_p (tr + i ti)(ur + i ui), scaled by E dV per channel.
+template <int SB, int NCH>
+__global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X, long long ldx, long long xim, int ns,
+                                                   const int* __restrict__ atom_off, const int* __restrict__ pt_g,
+                                                   const double* __restrict__ ztab, long long npts,
+                                                   const double* __restrict__ ch_scale, double* __restrict__ coef,
+                                                   int ncoef) {
+    const int atom = blockIdx.x;
+    const int s0 = blockIdx.y * SB;
+    const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
+    double ar[SB][NCH], ai[SB][NCH];
+#pragma unroll
+    for (int s = 0; s < SB; ++s)
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) ar[s][c] = ai[s][c] = 0.0;
+    const double* Xs[SB];
+#pragma unroll
+    for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
+
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        const int g = pt_g[p];
+        double tr[NCH], ti[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            tr[c] = ztab[(long long)c * npts + p];
+            ti[c] = ztab[(long long)(NCH + c) * npts + p];
+        }
+#pragma unroll
+        for (int s = 0; s < SB; ++s) {
+            const double ur = Xs[s][g], ui = Xs[s][xim + g];
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+                ar[s][c] += tr[c] * ur - ti[c] * ui;
+                ai[s][c] += ti[c] * ur + tr[c] * ui;
+            }
+        }
+    }
+    __shared__ double red[8][2 * SB * NCH];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < SB; ++s)
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            double vr = ar[s][c], vi = ai[s][c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                vr += __shfl_xor_sync(0xffffffffu, vr, o);
+                vi += __shfl_xor_sync(0xffffffffu, vi, o);
+            }
+            if (lane == 0) {
+                red[warp][2 * (s * NCH + c)] = vr;
+                red[warp][2 * (s * NCH + c) + 1] = vi;
+            }
+        }
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < 2 * SB * NCH; i += blockDim.x) {
+        double v = 0.0;
+        for (int w = 0; w < nw; ++w) v += red[w][i];
+        const int sc = i >> 1, s = sc / NCH, c = sc % NCH;
+        if (s0 + s < ns) coef[((long long)(s0 + s) * ncoef + atom * NCH + c) * 2 + (i & 1)] = ch_scale[atom * NCH + c] * v;
+    }
+}
+
+// Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[s][a_e, ch].
+template <int SG, int NCH>
+__global__ void __launch_bounds__(256) k_scatter_all_z(double* __restrict__ HX, long long ldhx, long long hxim, int ns,
+                                                       long long N, const int* __restrict__ row,
+                                                       const int* __restrict__ ent_atom,
+                                                       const double* __restrict__ zent,
+                                                       const double* __restrict__ coef, int ncoef) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    const int e0 = row[g], e1 = row[g + 1];
+    if (e0 == e1) return;
+    for (int s0 = 0; s0 < ns; s0 += SG) {
+        const int gn = min(SG, ns - s0);
+        double accr[SG], acci[SG];
+#pragma unroll
+        for (int s = 0; s < SG; ++s) accr[s] = acci[s] = 0.0;
+        const double* cg = coef + (long long)s0 * ncoef * 2;
+        for (int e = e0; e < e1; ++e) {
+            const int base = __ldg(&ent_atom[e]) * NCH;
+            double vr[NCH], vi[NCH];
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+                vr[c] = __ldg(&zent[((long long)e * NCH + c) * 2]);
+                vi[c] = __ldg(&zent[((long long)e * NCH + c) * 2 + 1]);
+            }
+#pragma unroll
+            for (int s = 0; s < SG; ++s) {
+                if (s < gn) {
+#pragma unroll
+                    for (int c = 0; c < NCH; ++c) {
+                        const double cr = __ldg(&cg[((long long)s * ncoef + base + c) * 2]);
+                        const double ci = __ldg(&cg[((long long)s * ncoef + base + c) * 2 + 1]);
+                        accr[s] += vr[c] * cr + vi[c] * ci;
+                        acci[s] += vr[c] * ci - vi[c] * cr;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < SG; ++s)
+            if (s < gn) {
+                double* hr = HX + (long long)(s0 + s) * ldhx + g;
+                hr[0] += accr[s];
+                hr[hxim] += acci[s];
+            }
+    }
+}
+
+// Any-shape fallback for V u - 1/2 (Lap + 2i g.grad - g^2) u: one thread per
+// (point, state), neighbours read from global memory with periodic wrap.
+__global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<double> a) {
+    const long long N = (long long)a.nx * a.ny * a.nz;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int s = blockIdx.y;
+    const int ix = (int)(i % a.nx), iy = (int)((i / a.nx) % a.ny), iz = (int)(i / ((long long)a.nx * a.ny));
+    double lap[2], der[2], cen[2];
+    for (int c = 0; c < 2; ++c) {
+        const double* u = a.X + (long long)s * a.ldx + (c ? a.xim : 0);
+        auto at = [&](int dx, int dy, int dz) {
+            return u[wrap_idx(ix + dx, a.nx) + (long long)a.nx * (wrap_idx(iy + dy, a.ny) + (long long)a.ny * wrap_idx(iz + dz, a.nz))];
+        };
+        double xm[4], xp[4], ym[4], yp[4], zm[4], zp[4];
+        for (int d = 1; d <= 4; ++d) {
+            xm[d - 1] = at(-d, 0, 0); xp[d - 1] = at(d, 0, 0);
+            ym[d - 1] = at(0, -d, 0); yp[d - 1] = at(0, d, 0);
+            zm[d - 1] = at(0, 0, -d); zp[d - 1] = at(0, 0, d);
+        }
+        cen[c] = u[i];
+        double l = a.c0 * cen[c];
+        l += a.cx[3] * (xp[3] + xm[3]) + a.cx[2] * (xp[2] + xm[2]) + a.cx[1] * (xp[1] + xm[1]) + a.cx[0] * (xp[0] + xm[0]);
+        l += a.cy[3] * (yp[3] + ym[3]) + a.cy[2] * (yp[2] + ym[2]) + a.cy[1] * (yp[1] + ym[1]) + a.cy[0] * (yp[0] + ym[0]);
+        l += a.cz[3] * (zp[3] + zm[3]) + a.cz[2] * (zp[2] + zm[2]) + a.cz[1] * (zp[1] + zm[1]) + a.cz[0] * (zp[0] + zm[0]);
+        lap[c] = l;
+        double g = a.dx[3] * (xp[3] - xm[3]) + a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
+        g += a.dy[3] * (yp[3] - ym[3]) + a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
+        g += a.dz[3] * (zp[3] - zm[3]) + a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
+        der[c] = g;
+    }
+    const double v = a.V[i];
+    double* h = a.HX + (long long)s * a.ldhx + i;
+    h[0] = (v * cen[0] + lap[0]) - der[1];
+    h[a.hxim] = (v * cen[1] + lap[1]) + der[0];
+}
+
+template <int NCH>
+void launch_project_z_nch(const DevProjectors& pj, int ns, const double* X, long long ldx, long long xim,
+                          double* coef, cudaStream_t st) {
+    if (pj.na * ((ns + 3) / 4) >= 2 * 148) {
+        dim3 g(pj.na, (ns + 3) / 4);
+        k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
+                                               coef, pj.na * NCH);
+    } else if (pj.na * ((ns + 1) / 2) >= 2 * 148) {
+        dim3 g(pj.na, (ns + 1) / 2);
+        k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
+                                               coef, pj.na * NCH);
+    } else {
+        dim3 g(pj.na, ns);
+        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
+                                               coef, pj.na * NCH);
+    }
+}
+
+template <int NCH>
+void launch_scatter_z_nch(const DevProjectors& pj, double* HX, long long ldhx, long long hxim, int ns, long long N,
+                          const double* coef, cudaStream_t st) {
+    k_scatter_all_z<4, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(HX, ldhx, hxim, ns, N, pj.row, pj.ent_atom,
+                                                                         pj.zent, coef, pj.na * NCH);
+}
+
+// Bloch-phase tables for the operator's current k-vector.
+int ensure_bloch_tables(qg_hamiltonian h, cudaStream_t st) {
+    DevProjectors& pj = h->pj;
+    if (pj.na <= 0 || pj.nch <= 0) return QG_OK;
+    if (pj.zready && pj.zg[0] == h->gx && pj.zg[1] == h->gy && pj.zg[2] == h->gz) return QG_OK;
+    if (!pj.ztab) {
+        QG_CUDA_TRY(cudaMalloc(&pj.ztab, (size_t)2 * pj.nch * pj.npts * sizeof(double)));
+        QG_CUDA_TRY(cudaMalloc(&pj.zent, (size_t)2 * pj.nch * pj.nent * sizeof(double)));
+    }
+    const long long total = pj.npts + pj.nent;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_bloch_tables<<<blocks, 256, 0, st>>>(pj.tab_d, pj.pt_u, pj.npts, pj.ent_pt, pj.nent, pj.nch, h->gx * h->hx,
+                                           h->gy * h->hy, h->gz * h->hz, pj.ztab, pj.zent);
+    QG_CUDA_TRY(cudaGetLastError());
+    pj.zg[0] = h->gx; pj.zg[1] = h->gy; pj.zg[2] = h->gz;
+    pj.zready = true;
+    return QG_OK;
+}
+
+}  // namespace
+
+int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
+                        double* coef, cudaStream_t st, PhaseTimer* pt) {
+    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    const DevProjectors& pj = h->pj;
+    const long long N = h->N();
+    HamArgs<double> a{};
+    a.X = X; a.ldx = ldx; a.HX = HX; a.ldhx = ldhx; a.ns = ns;
+    a.xim = N; a.hxim = N;
+    a.V = h->V_d;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.ty = h->ty;
+    a.err = h->ctx->dev_status;
+    // -1/2 (Lap + 2i g.grad - g^2) exactly as LaplasianKpoint8th_halo_f forms it
+    const double coefk = -0.5;
+    const double hh[3] = {h->hx, h->hy, h->hz};
+    const double gg[3] = {h->gx, h->gy, h->gz};
+    double* cs[3] = {a.cx, a.cy, a.cz};
+    double* ds[3] = {a.dx, a.dy, a.dz};
+    a.c0 = -14350.0 / 5040.0 * coefk * (1.0 / (hh[0] * hh[0]) + 1.0 / (hh[1] * hh[1]) + 1.0 / (hh[2] * hh[2])) -
+           coefk * (gg[0] * gg[0] + gg[1] * gg[1] + gg[2] * gg[2]);
+    const double coef2 = coefk * 2.0;
+    for (int d = 0; d < 3; ++d) {
+        const double s = 5040.0 * hh[d] * hh[d];
+        cs[d][3] = -9.0 * coefk / s;
+        cs[d][2] = 128.0 * coefk / s;
+        cs[d][1] = -1008.0 * coefk / s;
+        cs[d][0] = 8064.0 * coefk / s;
+        const bool on = std::fabs(gg[d]) >= 1.0e-8;  // LaplasianKpoint8th_ddm skips |g| < 1e-8
+        ds[d][0] = on ? 672.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
+        ds[d][1] = on ? -168.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
+        ds[d][2] = on ? 32.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
+        ds[d][3] = on ? -3.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
+    }
+    const bool nonlocal = pj.na > 0 && pj.nch > 0;
+    if (pt) pt->mark(0, st);
+    if (nonlocal) {
+        QG_TRY(ensure_bloch_tables(h, st));
+        switch (pj.nch) {
+            case 4: launch_project_z_nch<4>(pj, ns, X, ldx, N, coef, st); break;
+            case 8: launch_project_z_nch<8>(pj, ns, X, ldx, N, coef, st); break;
+            case 16: launch_project_z_nch<16>(pj, ns, X, ldx, N, coef, st); break;
+            default: return QG_ERR_UNSUPPORTED;
+        }
+    }
+    if (pt) pt->mark(1, st);
+    if (h->force_plain_stencil || !stencil_tma_ok<double>(a, 8, 2)) {
+        dim3 g((unsigned)((N + 255) / 256), (unsigned)ns);
+        k_kpoint_plain<<<g, 256, 0, st>>>(a);
+    } else {
+        QG_TRY(launch_stencil_tma<double>(a, 8, st, 2));
+    }
+    if (pt) pt->mark(2, st);
+    if (nonlocal) {
+        switch (pj.nch) {
+            case 4: launch_scatter_z_nch<4>(pj, HX, ldhx, N, ns, N, coef, st); break;
+            case 8: launch_scatter_z_nch<8>(pj, HX, ldhx, N, ns, N, coef, st); break;
+            default: launch_scatter_z_nch<16>(pj, HX, ldhx, N, ns, N, coef, st); break;
+        }
+    }
+    if (pt) pt->mark(-1, st);
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
+
+}  // namespace qg
+
+namespace {
+
+int apply_z_checked(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx) {
+    if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
+    if (ns == 0) return QG_OK;
+    const long long N = h->N();
+    if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
+    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    double* coef = nullptr;
+    if (h->pj.na > 0) {
+        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, ns) * sizeof(double)));
+        coef = h->coef.as<double>();
+    }
+    return qg::apply_hamiltonian_z(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int qg_hamiltonian_apply_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx) {
+    return apply_z_checked(h, ns, X, ldx, HX, ldhx);
+}
+
+int qg_hamiltonian_apply_timed_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX,
+                                 long long ldhx, float* ms_phases) {
+    if (!h || ns <= 0 || !X || !HX || !ms_phases) return QG_ERR_INVALID;
+    const long long N = h->N();
+    if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
+    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    double* coef = nullptr;
+    if (h->pj.na > 0) {
+        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, ns) * sizeof(double)));
+        coef = h->coef.as<double>();
+    }
+    qg::PhaseTimer pt;
+    QG_TRY(qg::apply_hamiltonian_z(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream, &pt));
+    pt.totals(ms_phases);
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
+
+int qg_hamiltonian_apply_host_z(qg_hamiltonian h, int ns, const double* X, double* HX) {
+    if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
+    if (ns == 0) return QG_OK;
+    const long long N = h->N();
+    const size_t bytes = (size_t)ns * 2 * N * sizeof(double);
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    QG_TRY(h->xio.reserve(bytes));
+    QG_TRY(h->hxio.reserve(bytes));
+    cudaStream_t st = h->ctx->stream;
+    QG_CUDA_TRY(cudaMemcpyAsync(h->xio.ptr, X, bytes, cudaMemcpyHostToDevice, st));
+    QG_TRY(apply_z_checked(h, ns, h->xio.as<double>(), 2 * N, h->hxio.as<double>(), 2 * N));
+    QG_CUDA_TRY(cudaMemcpyAsync(HX, h->hxio.ptr, bytes, cudaMemcpyDeviceToHost, st));
+    QG_CUDA_TRY(cudaStreamSynchronize(st));
+    return QG_OK;
+}
+
+}  // extern "C"

@@ -73,6 +73,18 @@ struct DevProjectors {
     int* ent_atom = nullptr;
     double* ent_val_d = nullptr;
     float* ent_val_f = nullptr;
+    // k-point (complex) side: unwrapped grid coordinates of each point (3 per
+    // point, the image the cube point came from), the point of each scatter
+    // entry, and the Bloch-phase tables for the k-vector zg:
+    //   ztab[ch*npts + p] = tab * cos(theta_p), ztab[(nch + ch)*npts + p] = tab * sin(theta_p),
+    //   zent[(e*nch + ch)*2 + {0,1}] = ent_val * (cos, sin)(theta_p(e)),
+    // theta_p = g . (h * u_p)
+    int* pt_u = nullptr;
+    int* ent_pt = nullptr;
+    double* ztab = nullptr;
+    double* zent = nullptr;
+    double zg[3] = {0, 0, 0};
+    bool zready = false;
 };
 
 namespace qg {
@@ -135,5 +147,10 @@ size_t coef_scratch_elems(qg_hamiltonian h, int ns);
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
                       T* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
+
+// Complex k-point H (kpoint.cu): state s has its real part at X + s*ldx and its
+// imaginary part N elements later; coef_scratch holds 2*coef_scratch_elems(h, ns) doubles.
+int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
+                        double* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
 
 }  // namespace qg

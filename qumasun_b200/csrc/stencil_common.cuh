@@ -25,6 +25,12 @@ struct HamArgs {
     int ncoef;       // na * nch
     const T* coef;   // [ns][ncoef]
     int* err;        // device status word: nonzero after a bounded wait gave up
+    // complex (k-point) states: the imaginary part of a state starts xim (hxim)
+    // elements after its real part; dx/dy/dz are the 8th-order first-derivative
+    // coefficients 2*coef*g/(840h)*(672, -168, 32, -3) per axis (zero for an
+    // axis whose |g| < 1e-8), c0 then carries the -coef*|g|^2 term
+    long long xim, hxim;
+    T dx[4], dy[4], dz[4];
 };
 
 __device__ __forceinline__ int wrap_idx(int i, int n) {
@@ -33,10 +39,11 @@ __device__ __forceinline__ int wrap_idx(int i, int n) {
 }
 
 
+// nc = 1: real states; nc = 2: complex k-point states (order 8 only).
 template <typename T>
-int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st);
+int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc = 1);
 // True when launch_stencil_tma accepts this shape and alignment.
 template <typename T>
-bool stencil_tma_ok(const HamArgs<T>& a, int order);
+bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc = 1);
 
 }  // namespace qg

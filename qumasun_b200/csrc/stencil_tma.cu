@@ -120,9 +120,23 @@ __device__ __forceinline__ T lap_point(T c, const T* xm, const T* xp, const T* y
     }
 }
 
+// g.grad of one point with the 8th-order first derivative (672, -168, 32, -3)/840h,
+// grouped as in LaplasianKpoint8th_halo_f (GridDifferenceKpoint8th.h:18-122); the
+// factor 2*coef and g are folded into a.dx/dy/dz.
+template <typename T>
+__device__ __forceinline__ T der_point(const T* xm, const T* xp, const T* ym, const T* yp, const T* zm,
+                                       const T* zp, const HamArgs<T>& a) {
+    T g = a.dx[3] * (xp[3] - xm[3]) + a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
+    g += a.dy[3] * (yp[3] - ym[3]) + a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
+    g += a.dz[3] * (zp[3] - zm[3]) + a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
+    return g;
+}
+
 constexpr int kBarBytes = 1024;  // mbarriers + control words at the front of dynamic shared memory
 constexpr int kMaxThreads = 416;
 constexpr int kMaxConsumers = 384;
+constexpr int kMaxThreadsKp = 288;  // complex states keep two register windows per thread
+constexpr int kMaxConsumersKp = 256;
 constexpr int kMaxStages = 16;
 
 template <int ORDER>
@@ -138,9 +152,13 @@ struct WorkGrid {
 // Persistent kernel: block b processes work items b, b + gridDim.x, ... where
 // item = (state, y tile, z slab). The plane ring and its phases run on across
 // items, so the producer streams the next item's planes while the consumers
-// finish the current one.
-template <typename T, int ORDER, int PX>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T> a, const WorkGrid wg, int nst) {
+// finish the current one. NC = 2 carries complex k-point states: a stage holds
+// the real and the imaginary rows of one plane, and each point adds the
+// first-derivative coupling -(1/2) 2i g.grad between the two parts
+// (LaplasianKpoint8th_halo_f, GridDifferenceKpoint8th.h:18-122).
+template <typename T, int ORDER, int PX, int NC>
+__global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
+    k_stencil_tma(const HamArgs<T> a, const WorkGrid wg, int nst) {
     constexpr int R = radius<ORDER>();
     constexpr int Q = 2 * R + 1;
     constexpr int NV = (R + PX - 1) / PX;  // neighbour vectors each side in x
@@ -153,7 +171,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
 
     const int nx = a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
     const int rows = ty + 2 * R;
-    const int stage_elems = rows * nx;
+    const int comp_elems = rows * nx;  // one part (real or imaginary) of a plane
+    const int stage_elems = NC * comp_elems;
     const uint32_t stage_bytes = (uint32_t)stage_elems * sizeof(T);
     const int tpr = nx / PX;
     const int ncons = tpr * ty;
@@ -196,13 +215,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
                     const long long zoff = (long long)wrap_idx(p, nz) * plane;
                     T* dst = ring + (size_t)j * stage_elems;
                     mbar_expect_tx(&full[j], stage_bytes);
-                    int r = 0;
-                    while (r < rows) {
-                        const int y = wrap_idx(y0 - R + r, ny);
-                        const int cnt = min(rows - r, ny - y);
-                        bulk_g2s(dst + (size_t)r * nx, Xs + zoff + (long long)y * nx, (uint32_t)(cnt * nx * sizeof(T)),
-                                 &full[j]);
-                        r += cnt;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const T* src = Xs + (c ? a.xim : 0) + zoff;
+                        int r = 0;
+                        while (r < rows) {
+                            const int y = wrap_idx(y0 - R + r, ny);
+                            const int cnt = min(rows - r, ny - y);
+                            bulk_g2s(dst + (size_t)c * comp_elems + (size_t)r * nx, src + (long long)y * nx,
+                                     (uint32_t)(cnt * nx * sizeof(T)), &full[j]);
+                            r += cnt;
+                        }
                     }
                     ctl[1] = pos;
                 }
@@ -237,7 +260,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
             const int ze = min(nz, zs + wg.zslab);
             const long long col = (long long)iy * nx + ix0;
 
-            Vec<T, PX> q[Q];
+            Vec<T, PX> q[NC][Q];
             Vec<T, PX> vq[R + 1];  // V of planes z .. z+R
             // prologue: own z-window from the item's first 2R planes
             int j = pos % nst;
@@ -246,7 +269,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
 #pragma unroll
             for (int d = 0; d < 2 * R; ++d) {
                 if (w && !mbar_wait(&full[j], ph)) w = false;
-                q[d].v = *reinterpret_cast<const VT*>(ring + j * stage_elems + rowoff + ix0);
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+                    q[cc][d].v = *reinterpret_cast<const VT*>(ring + j * stage_elems + cc * comp_elems + rowoff + ix0);
                 if (++j == nst) { j = 0; ph ^= 1u; }
             }
             const T* vp = a.V + (long long)zs * plane + col;  // no wrap: zslab >= 2R keeps zs + R - 1 < ze <= nz
@@ -276,49 +301,68 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
                     bad = true;
                     break;
                 }
-                const T* pzs = ring + jz * stage_elems;
-                const T* pps = ring + jp * stage_elems;
-                q[2 * R].v = *reinterpret_cast<const VT*>(pps + rowoff + ix0);
-                T xv[(2 * NV + 1) * PX];
+                T lap[NC][PX], der[NC][PX];
 #pragma unroll
-                for (int v = 0; v < 2 * NV; ++v) {
-                    Vec<T, PX> wv;
-                    wv.v = *reinterpret_cast<const VT*>(pzs + xoff[v]);
-                    const int slot = (v < NV) ? v : v + 1;
+                for (int cc = 0; cc < NC; ++cc) {
+                    const T* pzs = ring + jz * stage_elems + cc * comp_elems;
+                    const T* pps = ring + jp * stage_elems + cc * comp_elems;
+                    q[cc][2 * R].v = *reinterpret_cast<const VT*>(pps + rowoff + ix0);
+                    T xv[(2 * NV + 1) * PX];
 #pragma unroll
-                    for (int e = 0; e < PX; ++e) xv[slot * PX + e] = wv.e[e];
-                }
+                    for (int v = 0; v < 2 * NV; ++v) {
+                        Vec<T, PX> wv;
+                        wv.v = *reinterpret_cast<const VT*>(pzs + xoff[v]);
+                        const int slot = (v < NV) ? v : v + 1;
 #pragma unroll
-                for (int e = 0; e < PX; ++e) xv[NV * PX + e] = q[R].e[e];
-                Vec<T, PX> ypv[R], ymv[R];
+                        for (int e = 0; e < PX; ++e) xv[slot * PX + e] = wv.e[e];
+                    }
 #pragma unroll
-                for (int d = 1; d <= R; ++d) {
-                    ypv[d - 1].v = *reinterpret_cast<const VT*>(pzs + rowoff + ix0 + d * nx);
-                    ymv[d - 1].v = *reinterpret_cast<const VT*>(pzs + rowoff + ix0 - d * nx);
+                    for (int e = 0; e < PX; ++e) xv[NV * PX + e] = q[cc][R].e[e];
+                    Vec<T, PX> ypv[R], ymv[R];
+#pragma unroll
+                    for (int d = 1; d <= R; ++d) {
+                        ypv[d - 1].v = *reinterpret_cast<const VT*>(pzs + rowoff + ix0 + d * nx);
+                        ymv[d - 1].v = *reinterpret_cast<const VT*>(pzs + rowoff + ix0 - d * nx);
+                    }
+#pragma unroll
+                    for (int e = 0; e < PX; ++e) {
+                        T xm[R], xp[R], ym[R], yp[R], zm[R], zp[R];
+#pragma unroll
+                        for (int d = 1; d <= R; ++d) {
+                            xm[d - 1] = xv[NV * PX + e - d];
+                            xp[d - 1] = xv[NV * PX + e + d];
+                            ym[d - 1] = ymv[d - 1].e[e];
+                            yp[d - 1] = ypv[d - 1].e[e];
+                            zm[d - 1] = q[cc][R - d].e[e];
+                            zp[d - 1] = q[cc][R + d].e[e];
+                        }
+                        lap[cc][e] = lap_point<T, ORDER>(q[cc][R].e[e], xm, xp, ym, yp, zm, zp, a);
+                        if constexpr (NC == 2) der[cc][e] = der_point<T>(xm, xp, ym, yp, zm, zp, a);
+                    }
                 }
                 __syncwarp(wmask);
                 if (lane == 0) mbar_arrive(&empty[jz]);  // plane z is no longer read
-                Vec<T, PX> out;
+                if constexpr (NC == 1) {
+                    Vec<T, PX> out;
 #pragma unroll
-                for (int e = 0; e < PX; ++e) {
-                    T xm[R], xp[R], ym[R], yp[R], zm[R], zp[R];
+                    for (int e = 0; e < PX; ++e) out.e[e] = vq[0].e[e] * q[0][R].e[e] + lap[0][e];
+                    *reinterpret_cast<VT*>(hxp) = out.v;
+                } else {
+                    // re: V re + L re - D im;  im: V im + L im + D re
+                    Vec<T, PX> ore, oim;
 #pragma unroll
-                    for (int d = 1; d <= R; ++d) {
-                        xm[d - 1] = xv[NV * PX + e - d];
-                        xp[d - 1] = xv[NV * PX + e + d];
-                        ym[d - 1] = ymv[d - 1].e[e];
-                        yp[d - 1] = ypv[d - 1].e[e];
-                        zm[d - 1] = q[R - d].e[e];
-                        zp[d - 1] = q[R + d].e[e];
+                    for (int e = 0; e < PX; ++e) {
+                        ore.e[e] = (vq[0].e[e] * q[0][R].e[e] + lap[0][e]) - der[1][e];
+                        oim.e[e] = (vq[0].e[e] * q[1][R].e[e] + lap[1][e]) + der[0][e];
                     }
-                    const T cc = q[R].e[e];
-                    const T lap = lap_point<T, ORDER>(cc, xm, xp, ym, yp, zm, zp, a);
-                    out.e[e] = vq[0].e[e] * cc + lap;
+                    *reinterpret_cast<VT*>(hxp) = ore.v;
+                    *reinterpret_cast<VT*>(hxp + a.hxim) = oim.v;
                 }
-                *reinterpret_cast<VT*>(hxp) = out.v;
                 hxp += plane;
 #pragma unroll
-                for (int d = 0; d < 2 * R; ++d) q[d] = q[d + 1];
+                for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+                    for (int d = 0; d < 2 * R; ++d) q[cc][d] = q[cc][d + 1];
 #pragma unroll
                 for (int d = 0; d < R; ++d) vq[d] = vq[d + 1];
                 if (++jz == nst) jz = 0;
@@ -346,13 +390,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_stencil_tma(const HamArgs<T>
     }
 }
 
-// Rows per tile: the largest divisor of ny (<= 16) keeping consumers + producer warp <= kMaxThreads.
+// Rows per tile: the largest divisor of ny (<= 16) keeping the consumer threads within the kernel's limit.
 template <typename T>
-int tma_tile_rows(const HamArgs<T>& a) {
+int tma_tile_rows(const HamArgs<T>& a, int nc) {
     constexpr int PX = 16 / sizeof(T);
+    const int maxc = nc == 1 ? kMaxConsumers : kMaxConsumersKp;
     int ty = 0;
     for (int t = 1; t <= 16; ++t)
-        if (a.ny % t == 0 && (a.nx / PX) * t <= kMaxConsumers) ty = t;
+        if (a.ny % t == 0 && (a.nx / PX) * t <= maxc) ty = t;
     return ty;
 }
 
@@ -375,20 +420,20 @@ int sm_count() {
     return n;
 }
 
-template <typename T, int ORDER>
+template <typename T, int ORDER, int NC>
 int launch_order(const HamArgs<T>& a, cudaStream_t st) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = radius<ORDER>();
-    const size_t stage = (size_t)(a.ty + 2 * R) * a.nx * sizeof(T);
+    const size_t stage = (size_t)NC * (a.ty + 2 * R) * a.nx * sizeof(T);
     const int nst = ring_stages_for(R, stage);
     if (nst < 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = kBarBytes + (size_t)nst * stage;
-    auto kern = k_stencil_tma<T, ORDER, PX>;
+    auto kern = k_stencil_tma<T, ORDER, PX, NC>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * a.ty;
     const int threads = 32 + ncons;
-    if (threads > kMaxThreads) return QG_ERR_UNSUPPORTED;
+    if (threads > (NC == 1 ? kMaxThreads : kMaxThreadsKp)) return QG_ERR_UNSUPPORTED;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
         return QG_ERR_UNSUPPORTED;
@@ -410,38 +455,44 @@ int launch_order(const HamArgs<T>& a, cudaStream_t st) {
 }  // namespace
 
 template <typename T>
-bool stencil_tma_ok(const HamArgs<T>& a, int order) {
+bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc) {
     constexpr int PX = 16 / sizeof(T);
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
+    if (nc != 1 && nc != 2) return false;
+    if (nc == 2 && (order != 8 || sizeof(T) != 8 || (a.xim % PX) || (a.hxim % PX))) return false;
     if (a.row) return false;  // the nonlocal scatter runs in k_scatter_all on this path
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R)
         return false;
-    const int ty = tma_tile_rows(a);
+    const int ty = tma_tile_rows(a, nc);
     if (ty == 0) return false;
-    const size_t stage = (size_t)(ty + 2 * R) * a.nx * sizeof(T);
+    const size_t stage = (size_t)nc * (ty + 2 * R) * a.nx * sizeof(T);
     return ring_stages_for(R, stage) > 0;
 }
 
 // Returns QG_ERR_UNSUPPORTED (launching nothing) when the shape or alignment
 // does not fit this kernel; the caller then uses the register-window kernel.
 template <typename T>
-int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st) {
-    if (!stencil_tma_ok<T>(a, order)) return QG_ERR_UNSUPPORTED;
+int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc) {
+    if (!stencil_tma_ok<T>(a, order, nc)) return QG_ERR_UNSUPPORTED;
     HamArgs<T> b = a;
-    b.ty = tma_tile_rows(a);
+    b.ty = tma_tile_rows(a, nc);
+    if (nc == 2) {
+        if constexpr (sizeof(T) == 8) return launch_order<T, 8, 2>(b, st);
+        return QG_ERR_UNSUPPORTED;
+    }
     switch (order) {
-        case 2: return launch_order<T, 2>(b, st);
-        case 4: return launch_order<T, 4>(b, st);
-        case 6: return launch_order<T, 6>(b, st);
-        case 8: return launch_order<T, 8>(b, st);
+        case 2: return launch_order<T, 2, 1>(b, st);
+        case 4: return launch_order<T, 4, 1>(b, st);
+        case 6: return launch_order<T, 6, 1>(b, st);
+        case 8: return launch_order<T, 8, 1>(b, st);
         default: return QG_ERR_INVALID;
     }
 }
 
-template bool stencil_tma_ok<double>(const HamArgs<double>&, int);
-template bool stencil_tma_ok<float>(const HamArgs<float>&, int);
-template int launch_stencil_tma<double>(const HamArgs<double>&, int, cudaStream_t);
-template int launch_stencil_tma<float>(const HamArgs<float>&, int, cudaStream_t);
+template bool stencil_tma_ok<double>(const HamArgs<double>&, int, int);
+template bool stencil_tma_ok<float>(const HamArgs<float>&, int, int);
+template int launch_stencil_tma<double>(const HamArgs<double>&, int, cudaStream_t, int);
+template int launch_stencil_tma<float>(const HamArgs<float>&, int, cudaStream_t, int);
 
 }  // namespace qg

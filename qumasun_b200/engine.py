@@ -107,6 +107,10 @@ def lib():
         L.qg_hamiltonian_apply_host_d.argtypes = [vp, C.c_int, vp, vp]
         L.qg_hamiltonian_apply_timed_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong,
                                                    C.POINTER(C.c_float)]
+        L.qg_hamiltonian_apply_z.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
+        L.qg_hamiltonian_apply_host_z.argtypes = [vp, C.c_int, vp, vp]
+        L.qg_hamiltonian_apply_timed_z.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong,
+                                                   C.POINTER(C.c_float)]
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_set_stencil_kernel.argtypes = [vp, C.c_int]
         L.qg_context_take_device_status.argtypes = [vp]
@@ -273,6 +277,39 @@ class Hamiltonian:
         check(lib().qg_hamiltonian_apply_timed_d(self.h, ns, C.c_void_p(x_ptr), self.N,
                                                  C.c_void_p(hx_ptr), self.N, ph),
               "qg_hamiltonian_apply_timed_d")
+        return tuple(ph)
+
+    # ---- complex k-point operator: states are (ns, 2N) rows {re[N], im[N]}
+    def set_kvector(self, g):
+        check(lib().qg_hamiltonian_set_kvector(self.h, float(g[0]), float(g[1]), float(g[2])),
+              "qg_hamiltonian_set_kvector")
+
+    def apply_z(self, X, out=None):
+        """H_k X for a float64 torch CUDA tensor (ns, 2N) of split-complex states."""
+        import torch
+        assert X.is_cuda and X.dim() == 2 and X.shape[1] == 2 * self.N and X.dtype == torch.float64
+        X = X.contiguous()
+        if out is None:
+            out = torch.empty_like(X)
+        self.ctx.use_torch_stream()
+        check(lib().qg_hamiltonian_apply_z(self.h, X.shape[0], C.c_void_p(X.data_ptr()), 2 * self.N,
+                                           C.c_void_p(out.data_ptr()), 2 * self.N), "qg_hamiltonian_apply_z")
+        return out
+
+    def apply_host_z(self, X: np.ndarray, out: np.ndarray | None = None):
+        """H_k X with host buffers (ns, 2N)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        if out is None:
+            out = np.empty_like(X)
+        check(lib().qg_hamiltonian_apply_host_z(self.h, X.shape[0], X.ctypes.data, out.ctypes.data),
+              "qg_hamiltonian_apply_host_z")
+        return out
+
+    def apply_timed_z(self, ns, x_ptr, hx_ptr):
+        ph = (C.c_float * 3)()
+        check(lib().qg_hamiltonian_apply_timed_z(self.h, ns, C.c_void_p(x_ptr), 2 * self.N,
+                                                 C.c_void_p(hx_ptr), 2 * self.N, ph),
+              "qg_hamiltonian_apply_timed_z")
         return tuple(ph)
 
     def set_stencil_kernel(self, plain: bool):

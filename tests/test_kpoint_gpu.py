@@ -1,0 +1,122 @@
+"""Complex k-point H|psi> on the B200 against the reference's golden fixture
+(PseudoPotIntegrator_kpoint::ProjectionPP + LaplasianKpoint8th, run through
+oracle/_ref) and the CPU oracle. Tolerance: FP64 1e-12 relative per state
+(norm-wise) for the whole operator, and 1e-10 for the nonlocal part alone
+relative to its own size (it is ~4e-4 of the total on random states, so the
+subtraction of the local part costs about four digits)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from qumasun_b200.cell import build_cell, initial_states
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL64 = 1e-12
+KPOINT_CASES = {"noncubic": dict(grid=(20, 16, 24), displacement=0.05, seed=3),
+                "wrap": dict(grid=(12, 12, 12), a0=4.4)}
+
+
+def rel_per_state(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+
+
+def gpu_apply_z(ctx, cell, X, g, plain=False):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    H = Hamiltonian(ctx, cell, kvec=tuple(g))
+    H.set_stencil_kernel(plain)
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).to("cuda", torch.float64)
+    out = H.apply_z(Xd)
+    torch.cuda.synchronize()
+    H.close()
+    return out.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(GOLD, "ham_kpoint.npz"))
+
+
+@pytest.mark.parametrize("plain", [False, True], ids=["tma", "plain"])
+@pytest.mark.parametrize("name", sorted(KPOINT_CASES))
+def test_kpoint_matches_reference_golden(cuda_ctx, gold, name, plain):
+    cell = build_cell(**KPOINT_CASES[name])
+    X = gold[f"{name}_X"]
+    for i, g in enumerate(gold[f"{name}_g"]):
+        ref = gold[f"{name}_HX{i}"]
+        HX = gpu_apply_z(cuda_ctx, cell, X, g, plain)
+        assert rel_per_state(HX, ref).max() < TOL64, (name, i)
+        loc = O.hamiltonian_kpoint_local(cell, tuple(g), X)
+        assert rel_per_state(HX - loc, ref - loc).max() < 1e-10, (name, i)
+
+
+def test_kpoint_diamond8_general_k_and_kvector_switch(cuda_ctx):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell()  # 8 atoms, 40^3
+    X = initial_states(6, 2 * cell.N, seed=31)
+    g1 = (0.233, -0.466, 0.116)
+    g2 = (0.0, 0.233, 0.0)  # two components below the 1e-8 skip threshold
+    H = Hamiltonian(cuda_ctx, cell, kvec=g1)
+    Xd = torch.from_numpy(X).cuda()
+    a = H.apply_z(Xd).cpu().numpy()
+    H.set_kvector(g2)
+    b = H.apply_z(Xd).cpu().numpy()
+    hb = H.apply_host_z(X)
+    H.close()
+    assert rel_per_state(a, O.hamiltonian_kpoint_apply(cell, g1, X)).max() < TOL64
+    assert rel_per_state(b, O.hamiltonian_kpoint_apply(cell, g2, X)).max() < TOL64
+    np.testing.assert_array_equal(hb, b)
+
+
+def test_kpoint_gamma_equals_real_operator(cuda_ctx):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(grid=(24, 20, 16), displacement=0.1, seed=2)
+    N = cell.N
+    X = initial_states(3, 2 * N, seed=4)
+    H = Hamiltonian(cuda_ctx, cell)
+    z = H.apply_z(torch.from_numpy(X).cuda()).cpu().numpy()
+    r = H.apply(torch.from_numpy(X.reshape(6, N)).cuda()).cpu().numpy().reshape(3, 2 * N)
+    H.close()
+    assert rel_per_state(z, r).max() < 1e-14
+
+
+def test_kpoint_operator_is_hermitian_on_device(cuda_ctx):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell()
+    N = cell.N
+    X = initial_states(2, 2 * N, seed=5)
+    H = Hamiltonian(cuda_ctx, cell, kvec=(0.3, 0.2, -0.1))
+    HX = H.apply_z(torch.from_numpy(X).cuda()).cpu().numpy()
+    H.close()
+    z = X[:, :N] + 1j * X[:, N:]
+    hz = HX[:, :N] + 1j * HX[:, N:]
+    a = np.vdot(z[0], hz[1])
+    b = np.conj(np.vdot(z[1], hz[0]))
+    assert abs(a - b) < 1e-12 * abs(a)
+
+
+def test_kpoint_invalid_arguments(cuda_ctx):
+    import ctypes as C
+    import torch
+    from qumasun_b200 import Hamiltonian
+    from qumasun_b200.engine import lib
+    cell = build_cell(grid=(16, 16, 16))
+    H = Hamiltonian(cuda_ctx, cell, kvec=(0.1, 0.0, 0.0))
+    X = torch.zeros((2, 2 * cell.N), dtype=torch.float64, device="cuda")
+    Y = torch.empty_like(X)
+    assert lib().qg_hamiltonian_apply_z(H.h, 2, C.c_void_p(X.data_ptr()), cell.N, C.c_void_p(Y.data_ptr()),
+                                        2 * cell.N) == -1
+    # the real entry point refuses a nonzero Bloch vector
+    assert lib().qg_hamiltonian_apply_d(H.h, 2, C.c_void_p(X.data_ptr()), cell.N, C.c_void_p(Y.data_ptr()),
+                                        cell.N) == -1
+    H.close()
+    H6 = Hamiltonian(cuda_ctx, cell, fd_order=6, kvec=(0.1, 0.0, 0.0))
+    assert lib().qg_hamiltonian_apply_z(H6.h, 2, C.c_void_p(X.data_ptr()), 2 * cell.N, C.c_void_p(Y.data_ptr()),
+                                        2 * cell.N) == -7
+    H6.close()
