@@ -214,6 +214,22 @@ int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double
 int qg_lobpcg_d_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
                        double* X, double* P, qg_lobpcg_report* report);
 
+/* Complex block LOBPCG for the k-point operator (qg_hamiltonian_apply_z) on ns
+ * split-complex states: X and P are ns * 2N HOST doubles, state s = {re[N], im[N]}
+ * at X + 2Ns. Same iteration, options, stopping rule (max_j |r_j|^2 dV < tol dV)
+ * and statuses as qg_lobpcg_d; the Gram products are real DGEMMs over the re/im
+ * columns combined into the Hermitian pencil S = (RR + II) + i (RI - IR), solved
+ * in FP64 by cusolverDnZhegvd after Jacobi equilibration. The kinetic
+ * preconditioner (precond = 1) applies the Gamma-point FD symbol to the real and
+ * the imaginary part. Replaces LOBPCG::Eigen_z_multi_mpi (lobpcg_z_multi_mpi.h:988-1800:
+ * MakeMatrix_z_blas :214-300, lapack_ZHEGVX w_zhegvx.h:24-107, NextVector_z :586-712)
+ * as called by qumasun_kpoint.lobpcg.h:32-41. */
+int qg_lobpcg_z(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
+                double* P, qg_lobpcg_report* report);
+/* Same with DEVICE buffers X and P (ld = 2N); ev stays a host array. */
+int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
+                       double* X, double* P, qg_lobpcg_report* report);
+
 /* Batched small generalised eigensolver, FP64, DEVICE pointers, context stream:
  * for b < batch, A_b z = lambda B_b z with A_b = A + b*stride, B_b = B + b*stride
  * (k x k, column-major, leading dimension lda, lower triangles read), all k

@@ -126,6 +126,8 @@ def ref_lib():
         lib.ref_ylm_cube.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp]
         lib.ref_hamiltonian_kpoint_apply.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
                                                      C.c_double, C.c_double, C.c_int, _dp, _dp]
+        lib.ref_lobpcg_z_multi.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.c_int, C.c_int, _dp, _dp, C.c_int, _ip]
         _ref = lib
     return _ref
 
@@ -216,6 +218,37 @@ def ref_lobpcg_d_multi(cell, X0, iter_max, P0=None, first=True, quiet=True):
                                  _ptr(P, _dp), 1 if first else 0, 1 if quiet else 0,
                                  C.byref(iters))
     return dict(ev=ev, X=X, P=P, iters=iters.value, seconds=time.perf_counter() - t0)
+
+
+def ref_lobpcg_z_multi(cell, g, X0, iter_max, quiet=True):
+    """The reference's complex Eigen_z_multi_mpi (one rank, SCF step 0) with the reference
+    k-point H; X0 (ns, 2N) {re, im} states is not modified."""
+    X = _c64(X0).copy()
+    ns = X.shape[0]
+    ev = np.zeros(ns)
+    iters = C.c_int(0)
+    desc = HamDesc(cell, 8)
+    t0 = time.perf_counter()
+    rc = ref_lib().ref_lobpcg_z_multi(C.byref(desc.c), g[0], g[1], g[2], cell.cutoff, ns, iter_max,
+                                      _ptr(ev, _dp), _ptr(X, _dp), 1 if quiet else 0, C.byref(iters))
+    if rc != 0:
+        raise ValueError(f"ref_lobpcg_z_multi rejected ({rc})")
+    return dict(ev=ev, X=X, iters=iters.value, seconds=time.perf_counter() - t0)
+
+
+def dense_kpoint_hamiltonian(cell, g):
+    """The k-point H of the port as a dense complex N x N matrix (small grids only):
+    column j is H_k applied to the j-th unit vector."""
+    N = cell.N
+    H = np.zeros((N, N), dtype=np.complex128)
+    blk = 256
+    for j0 in range(0, N, blk):
+        j1 = min(N, j0 + blk)
+        X = np.zeros((j1 - j0, 2 * N))
+        X[np.arange(j1 - j0), np.arange(j0, j1)] = 1.0
+        HX = hamiltonian_kpoint_apply(cell, g, X)
+        H[:, j0:j1] = (HX[:, :N] + 1j * HX[:, N:]).T
+    return H
 
 
 def lobpcg_d_multi(apply_H, X0, dV, iter_max, limit=1.0e-10, P0=None, first=True, callback=None):

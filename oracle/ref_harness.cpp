@@ -16,6 +16,8 @@
  *                             zero, mPotentialMatrix (V*psi), ProjectionPP
  *                             (PseudoPotOperator.h:740-772), kinetic Laplacian (coef -1/2)
  *   ref_lobpcg_d_multi     -> EigenLOBPCG_d_multi (lobpcg_d_multi.h:23-545)
+ *   ref_lobpcg_z_multi     -> LOBPCG::Eigen_z_multi_mpi (lobpcg_z_multi_mpi.h:988-1800), one rank,
+ *                             with the reference k-point H as OpeA
  *   ref_grid_for_sphere    -> GridForSphere (GridSubgrid.h:482-492)
  *   ref_ylm_cube           -> SetYlmAround<L,M> (PseudoPotOperator.h:58-71)
  *   ref_hamiltonian_kpoint_apply
@@ -59,6 +61,8 @@ inline int lapack_DSYGVX(double* A, double* B, double* ev, double* evec, double*
     return lapack_DSYGVX(A, B, ev, evec, N);
 }
 #include "lobpcg_d_multi.h"
+#include "debug_print.h"
+#include "lobpcg_z_multi_mpi.h"
 
 /* PseudoPotIntegrator_single keeps its per-atom tables private; the harness
  * fills them directly instead of going through the .vps radial loader. */
@@ -453,6 +457,44 @@ int ref_hamiltonian_kpoint_apply(const ref_ham_desc* d, double gx, double gy, do
     const size_t N = (size_t)d->nx * d->ny * d->nz;
     for (int s = 0; s < ns; ++s)
         H.Apply(HX + (size_t)s * 2 * N, HX + (size_t)s * 2 * N + N, X + (size_t)s * 2 * N, X + (size_t)s * 2 * N + N);
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* The reference's complex block LOBPCG (Eigen_z_multi_mpi) on one rank with the
+ * reference k-point Hamiltonian as OpeA, SCF_step 0 (P starts from zero), run
+ * until its residual escape (max |r|^2 < LIMIT_Z_NORM_R_FOR_ESCAPE) or iter_max.
+ * X (ns * 2N, {re, im} per state) in/out, ev (ns) out; *iters receives the
+ * iterations taken (counted from OpeA calls). */
+int ref_lobpcg_z_multi(const ref_ham_desc* d, double gx, double gy, double gz, double rc, int ns, int iter_max,
+                       double* ev, double* X, int quiet, int* iters) {
+    if (d->fd_order != 8) return -1;
+    RefKpointHamiltonian H(d, gx, gy, gz, rc);
+    if (H.status) return H.status;
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    const double dV = d->hx * d->hy * d->hz;
+    std::vector<SoAComplex> evec(ns);
+    for (int s = 0; s < ns; ++s) {
+        evec[s].re = X + (size_t)s * 2 * N;
+        evec[s].im = X + (size_t)s * 2 * N + N;
+    }
+    std::vector<double> keep((size_t)ns * 2 * N, 0.0);
+    std::vector<double> work((size_t)5 * ns * 2 * N, 0.0);
+    long long calls = 0;
+    auto OpeA = [&](SoAComplex& Ax, const SoAComplex& x) {
+        ++calls;
+        H.Apply(Ax.re, Ax.im, x.re, x.im);
+    };
+    NullWatch watch;
+    {
+        QuietStdout q(quiet != 0);
+        LOBPCG::Eigen_z_multi_mpi(H.grid, dV, ns, iter_max, ev, evec.data(), keep.data(), work.data(),
+                                  (OneComplex*)nullptr, 0, 0, OpeA, watch);
+    }
+    if (iters) *iters = (int)((calls - 2LL * ns) / ns);
     return 0;
 }
 

@@ -41,6 +41,7 @@ typedef struct MPI_Status { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 #define MPI_FLOAT 4
 #define MPI_INT64_T 8
 #define MPI_UINT64_T 8
+#define MPI_UINT8_T 1
 #define MPI_LONG_LONG 8
 #define MPI_DOUBLE 8
 #define MPI_DOUBLE_COMPLEX 16

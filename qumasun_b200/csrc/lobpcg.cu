@@ -18,6 +18,7 @@
 // block per column and a fixed reduction order (deterministic).
 #include <cublas_v2.h>
 #include <cusolverDn.h>
+#include <cuComplex.h>
 
 #include <algorithm>
 #include <cmath>
@@ -162,6 +163,53 @@ __global__ void k_rowscale(double* __restrict__ Z, int ld, int k, const double* 
     }
 }
 
+// Complex Gram: S(i, j) = <w_i|A w_j> from the real Gram G = W^T AW of the split
+// layout (lobpcg_z_multi_mpi.h:214-300: S = (RR + II) + i (RI - IR)), Jacobi-
+// equilibrated by d = diag(B)^-1/2 like k_equilibrate; leading k x k block,
+// one block per column j.
+__global__ void k_gram_to_complex(const double* __restrict__ Ga, const double* __restrict__ Gb, int ldg, int k,
+                                  cuDoubleComplex* __restrict__ Ca, cuDoubleComplex* __restrict__ Cb, int ldc) {
+    const int j = blockIdx.x;
+    auto G = [ldg](const double* M, int r, int c) { return M[r + (long long)c * ldg]; };
+    auto dinv = [&](int i) {
+        const double b = G(Gb, 2 * i, 2 * i) + G(Gb, 2 * i + 1, 2 * i + 1);
+        return b > 0.0 ? 1.0 / sqrt(b) : 1.0;
+    };
+    const double dj = dinv(j);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const double s = dinv(i) * dj;
+        const double ar = G(Ga, 2 * i, 2 * j) + G(Ga, 2 * i + 1, 2 * j + 1);
+        const double ai = G(Ga, 2 * i, 2 * j + 1) - G(Ga, 2 * i + 1, 2 * j);
+        const double br = G(Gb, 2 * i, 2 * j) + G(Gb, 2 * i + 1, 2 * j + 1);
+        const double bi = G(Gb, 2 * i, 2 * j + 1) - G(Gb, 2 * i + 1, 2 * j);
+        Ca[i + (long long)j * ldc] = make_cuDoubleComplex(ar * s, ai * s);
+        Cb[i + (long long)j * ldc] = make_cuDoubleComplex(br * s, bi * s);
+    }
+}
+
+// Real rotation matrix of the split layout from the complex eigenvectors:
+// z = D z' (D as in k_gram_to_complex, rows >= krows zero), then
+// M(2i, 2j) = M(2i+1, 2j+1) = Re z(i, j), M(2i, 2j+1) = Im z(i, j), M(2i+1, 2j) = -Im z(i, j),
+// so that [re | im] columns times M give the complex product X z. One block per column j < n.
+__global__ void k_expand_rotation(const cuDoubleComplex* __restrict__ Z, int ldz, int k, int krows,
+                                  const double* __restrict__ Gb, int ldg, double* __restrict__ M, int ldm) {
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        double zr = 0.0, zi = 0.0;
+        if (i < krows) {
+            const double b = Gb[2 * i + (long long)(2 * i) * ldg] + Gb[2 * i + 1 + (long long)(2 * i + 1) * ldg];
+            const double d = b > 0.0 ? 1.0 / sqrt(b) : 1.0;
+            const cuDoubleComplex z = Z[i + (long long)j * ldz];
+            zr = cuCreal(z) * d;
+            zi = cuCimag(z) * d;
+        }
+        M[2 * i + (long long)(2 * j) * ldm] = zr;
+        M[2 * i + 1 + (long long)(2 * j + 1) * ldm] = zr;
+        M[2 * i + (long long)(2 * j + 1) * ldm] = zi;
+        M[2 * i + 1 + (long long)(2 * j) * ldm] = -zi;
+    }
+}
+
 struct Timer {
     cudaEvent_t ev[8];
     int n = 0;
@@ -191,17 +239,22 @@ struct Timer {
     }
 };
 
+// One LOBPCG instance. c = 1: real states (columns of N); c = 2: split-complex
+// states, each {re[N], im[N]} = two consecutive real columns, so every block is
+// also a real N x (c n) matrix for the Gram and rotation DGEMMs, and a state is
+// one contiguous "column" of L = c N values for norms, dots and residuals.
 struct Solver {
     qg_hamiltonian h;
-    int n;
-    long long N;
+    int n, c;
+    long long N, L;
     double dV;
     cudaStream_t st;
     cublasHandle_t blas;
     cusolverDnHandle_t sol;
     DevBuf W, AW, T, AT, S, small, work;
     int lwork = 0;
-    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb, *Sa2, *Sb2;
+    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb, *Sa2, *Sb2, *M;
+    cuDoubleComplex *Ca, *Cb;
     double *ev_d, *nr_d, *f_d, *f2_d, *w_d;
     int* info_d;
 
@@ -210,43 +263,66 @@ struct Solver {
     }
 
     int setup() {
-        const size_t blk = (size_t)N * n;
+        const size_t blk = (size_t)L * n;
         QG_TRY(W.reserve(3 * blk * sizeof(double)));
         QG_TRY(AW.reserve(3 * blk * sizeof(double)));
         QG_TRY(T.reserve(2 * blk * sizeof(double)));
         QG_TRY(AT.reserve(2 * blk * sizeof(double)));
-        const size_t k3 = 3 * (size_t)n;
-        QG_TRY(S.reserve(4 * k3 * k3 * sizeof(double)));
+        const size_t k3 = 3 * (size_t)n, g3 = c * k3;
+        // real Gram pair (c k3)^2 each; the equilibrated pencil (k3^2 real or complex each);
+        // for c = 2 the real rotation matrix (2 k3 x 2 n)
+        QG_TRY(S.reserve((2 * g3 * g3 + 2 * c * k3 * k3 + (c == 2 ? g3 * 2 * n : 0)) * sizeof(double)));
         QG_TRY(small.reserve((5 * k3 + 16) * sizeof(double)));
         x = W.as<double>(); r = x + blk; p = r + blk;
         Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
         Tx = T.as<double>(); Tp = Tx + blk;
         ATx = AT.as<double>(); ATp = ATx + blk;
-        Sa = S.as<double>(); Sb = Sa + k3 * k3; Sa2 = Sb + k3 * k3; Sb2 = Sa2 + k3 * k3;
+        Sa = S.as<double>(); Sb = Sa + g3 * g3; Sa2 = Sb + g3 * g3; Sb2 = Sa2 + c * k3 * k3;
+        M = Sb2 + c * k3 * k3;
+        // the triangle DSYRK(X) leaves unwritten stays finite (zero)
+        QG_CUDA_TRY(cudaMemsetAsync(S.ptr, 0, S.bytes, st));
+        Ca = reinterpret_cast<cuDoubleComplex*>(Sa2);
+        Cb = reinterpret_cast<cuDoubleComplex*>(Sb2);
         ev_d = small.as<double>(); nr_d = ev_d + k3; f_d = nr_d + k3; f2_d = f_d + k3; w_d = f2_d + k3;
         info_d = reinterpret_cast<int*>(w_d + k3);
-        QG_SOLVER_TRY(cusolverDnDsygvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                                  CUBLAS_FILL_MODE_LOWER, (int)k3, Sa, (int)k3, Sb, (int)k3, w_d,
-                                                  &lwork));
-        QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(double)));
-        QG_TRY(h->coef.reserve(qg::coef_scratch_elems(h, n) * sizeof(double)));
+        if (c == 1) {
+            QG_SOLVER_TRY(cusolverDnDsygvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                      CUBLAS_FILL_MODE_LOWER, (int)k3, Sa2, (int)k3, Sb2, (int)k3,
+                                                      w_d, &lwork));
+            QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(double)));
+        } else {
+            QG_SOLVER_TRY(cusolverDnZhegvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                      CUBLAS_FILL_MODE_LOWER, (int)k3, Ca, (int)k3, Cb, (int)k3,
+                                                      w_d, &lwork));
+            QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(cuDoubleComplex)));
+        }
+        QG_TRY(h->coef.reserve((size_t)c * qg::coef_scratch_elems(h, n) * sizeof(double)));
         return QG_OK;
     }
 
     int applyH(const double* in, double* out) {
-        return qg::apply_hamiltonian<double>(h, n, in, N, out, N, h->coef.as<double>(), st);
+        if (c == 1) return qg::apply_hamiltonian<double>(h, n, in, N, out, N, h->coef.as<double>(), st);
+        return qg::apply_hamiltonian_z(h, n, in, L, out, L, h->coef.as<double>(), st);
     }
 
     void coldot(const double* A, const double* B, double scale, double* out) {
-        k_coldot<<<n, kRedThreads, 0, st>>>(A, B, N, N, scale, out);
+        k_coldot<<<n, kRedThreads, 0, st>>>(A, B, L, L, scale, out);
     }
 
-    // scale columns of A (and B) by 1/sqrt(|A_j|^2 dV) computed from A
+    void scale_cols(double* A, double* B) {
+        dim3 g((unsigned)std::min<long long>((L + 255) / 256, 64), n);
+        k_scale_cols<<<g, 256, 0, st>>>(A, B, L, L, f_d);
+    }
+
+    // scale states of A (and B) by 1/sqrt(|A_j|^2 dV) computed from A
     void normalize(double* A, double* B) {
         coldot(A, A, 1.0, nr_d);
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(nr_d, dV, n, f_d);
-        dim3 g((unsigned)std::min<long long>((N + 255) / 256, 64), n);
-        k_scale_cols<<<g, 256, 0, st>>>(A, B, N, N, f_d);
+        scale_cols(A, B);
+    }
+
+    void residual() {
+        k_residual<<<n, kRedThreads, 0, st>>>(Ax, x, ev_d, r, L, L, dV, nr_d);
     }
 
     // C (m x nn, ldc) = alpha * A^T B, A: N x m, B: N x nn (ld N)
@@ -257,20 +333,69 @@ struct Solver {
         return QG_OK;
     }
 
-    // C (N x n) = A (N x k) * Z (k x n, ldz)
-    int gemm_nn(int k, const double* A, const double* Z, int ldz, double* C) {
+    // Sa = W^T AW dV, Sb = W^T W dV over the leading m real columns. For real
+    // states both are symmetric and only their lower triangles are formed
+    // (DSYRKX / DSYRK, half the flops; the eigensolvers read the lower triangle);
+    // the split-complex Gram is not symmetric column by column, so it takes full DGEMMs.
+    int gram(int m) {
+        if (c == 2) {
+            QG_TRY(gemm_tn(m, m, x, Ax, dV, Sa, m));
+            return gemm_tn(m, m, x, x, dV, Sb, m);
+        }
+        const double beta = 0.0;
+        QG_BLAS_TRY(cublasDsyrkx(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, m, (int)N, &dV, x, (int)N, Ax, (int)N,
+                                 &beta, Sa, m));
+        QG_BLAS_TRY(cublasDsyrk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, m, (int)N, &dV, x, (int)N, &beta, Sb, m));
+        return QG_OK;
+    }
+
+    // C (N x nc) = A (N x k) * Z (k x nc, ldz)
+    int gemm_nn(int k, int nc, const double* A, const double* Z, int ldz, double* C) {
         const double one = 1.0, zero = 0.0;
-        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, n, k, &one, A, (int)N, Z, ldz, &zero, C,
+        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nc, k, &one, A, (int)N, Z, ldz, &zero, C,
                                 (int)N));
+        return QG_OK;
+    }
+
+    // Small generalised eigenproblem on the leading k x k block of the Gram pair
+    // (row pitch k3), Jacobi-equilibrated; on success leaves the rotation matrix
+    // (the first n eigenvectors, back-scaled; rows >= krows zero) in *Zout/*ldz.
+    // Returns the solver's info (> 0: B not positive definite).
+    int solve_pencil(int k, int k3, int krows, const double** Zout, int* ldz, int* info) {
+        if (c == 1) {
+            k_equilibrate<<<k, 128, 0, st>>>(Sa, Sb, k3, k, Sa2, Sb2);
+            QG_SOLVER_TRY(cusolverDnDsygvd(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           k, Sa2, k3, Sb2, k3, w_d, work.as<double>(), lwork, info_d));
+        } else {
+            k_gram_to_complex<<<k, 128, 0, st>>>(Sa, Sb, 2 * k3, k, Ca, Cb, k3);
+            QG_SOLVER_TRY(cusolverDnZhegvd(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           k, Ca, k3, Cb, k3, w_d, work.as<cuDoubleComplex>(), lwork, info_d));
+        }
+        QG_CUDA_TRY(cudaMemcpyAsync(info, info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        if (*info != 0) return QG_OK;
+        if (c == 1) {
+            k_rowscale<<<n, 128, 0, st>>>(Sa2, k3, k, Sb, k3);  // z = D z'
+            if (krows < k3)
+                QG_CUDA_TRY(cudaMemset2DAsync(Sa2 + krows, (size_t)k3 * sizeof(double), 0,
+                                              (size_t)(k3 - krows) * sizeof(double), (size_t)n, st));
+            *Zout = Sa2;
+            *ldz = k3;
+        } else {
+            k_expand_rotation<<<n, 128, 0, st>>>(Ca, k3, k3, krows, Sb, 2 * k3, M, 2 * k3);
+            *Zout = M;
+            *ldz = 2 * k3;
+        }
         return QG_OK;
     }
 };
 
-int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev, double* X_dev, double* P_dev,
-               const double* X_host, double* Xout_host, const double* P_host, double* Pout_host,
+int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps, double* ev, double* X_dev,
+               double* P_dev, const double* X_host, double* Xout_host, const double* P_host, double* Pout_host,
                qg_lobpcg_report* rep) {
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
-    if (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0) return QG_ERR_INVALID;
+    if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
+    if (comps == 2 && h->order != 8) return QG_ERR_UNSUPPORTED;
     if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
     if (opt->precond != 0 && opt->precond != 1) return QG_ERR_INVALID;
     const long long N = h->N();
@@ -279,13 +404,15 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     Solver s;
     s.h = h;
     s.n = n;
+    s.c = comps;
     s.N = N;
+    s.L = comps * N;
     s.dV = h->hx * h->hy * h->hz;
     s.st = h->ctx->stream;
     QG_TRY(qg_blas_handle(h->ctx, &s.blas));
     QG_TRY(qg_solver_handle(h->ctx, &s.sol));
     QG_TRY(s.setup());
-    const size_t blk_bytes = (size_t)N * n * sizeof(double);
+    const size_t blk_bytes = (size_t)s.L * n * sizeof(double);
     const bool first = opt->first_call != 0;
     const double tol = opt->tol > 0 ? opt->tol : 1.0e-10;
     cudaStream_t st = s.st;
@@ -312,18 +439,19 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     if (first) QG_CUDA_TRY(cudaMemsetAsync(s.Ap, 0, blk_bytes, st));
     else QG_TRY(s.applyH(s.p, s.Ap));
     s.coldot(s.x, s.Ax, s.dV, s.ev_d);
-    k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
+    s.residual();
     qg::KineticPrecond* pc = nullptr;
     if (opt->precond == 1) {
+        // Gamma-point FD symbol on every real column (for k-point states it is an
+        // approximation of the k-shifted kinetic operator, still a valid preconditioner)
         if (!h->precond) h->precond = new qg::KineticPrecond();
         pc = h->precond;
-        QG_TRY(pc->setup(h, n, opt->precond_shift > 0 ? opt->precond_shift : 1.0));
+        QG_TRY(pc->setup(h, comps * n, opt->precond_shift > 0 ? opt->precond_shift : 1.0));
         QG_TRY(pc->apply(s.r, st));
         s.normalize(s.r, nullptr);
     } else {
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, 1.0, n, s.f_d);
-        dim3 g((unsigned)std::min<long long>((N + 255) / 256, 64), n);
-        k_scale_cols<<<g, 256, 0, st>>>(s.r, nullptr, N, N, s.f_d);
+        s.scale_cols(s.r, nullptr);
     }
     QG_CUDA_TRY(cudaGetLastError());
 
@@ -333,48 +461,35 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
     double maxres = 0.0;
     int status = QG_OK;
     int restarts = 0;
+    const int c = comps;
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
         tm.mark(1, st);
         const bool two = first && it == 0;
         const int k3 = (two ? 2 : 3) * n;
-        QG_TRY(s.gemm_tn(k3, k3, s.x, s.Ax, s.dV, s.Sa, k3));
-        QG_TRY(s.gemm_tn(k3, k3, s.x, s.x, s.dV, s.Sb, k3));
+        QG_TRY(s.gram(c * k3));
         tm.mark(2, st);
-        // Jacobi-equilibrated copy of the pencil (keeps the tiny residual columns of the
-        // reference iteration from ruining the Cholesky factor of B), cuSOLVER sygvd on it;
+        // Jacobi-equilibrated pencil (keeps the tiny residual columns of the reference
+        // iteration from ruining the Cholesky factor of B), cuSOLVER sygvd / hegvd on it;
         // if B is still not positive definite, restart this step without P
-        double* Z = s.Sa2;
+        const double* Z = nullptr;
+        int ldz = 0;
         bool restarted = false;
         int solve_info = 0;
-        k_equilibrate<<<k3, 128, 0, st>>>(s.Sa, s.Sb, k3, k3, s.Sa2, s.Sb2);
-        QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k3,
-                                       s.Sa2, k3, s.Sb2, k3, s.w_d, s.work.as<double>(), s.lwork, s.info_d));
-        QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
-        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        QG_TRY(s.solve_pencil(k3, k3, k3, &Z, &ldz, &solve_info));
         if (solve_info > 0 && k3 == 3 * n) {
             restarted = true;
-            if (k3 <= qg::kSmallEigMax) {
-                QG_TRY(qg::small_eig_launch(s.Sa, s.Sb, k3, 0, k3, 2 * n, Z, k3, 0, s.w_d, 0, s.info_d, 1, st));
+            if (c == 1 && k3 <= qg::kSmallEigMax) {
+                QG_TRY(qg::small_eig_launch(s.Sa, s.Sb, k3, 0, k3, 2 * n, s.Sa2, k3, 0, s.w_d, 0, s.info_d, 1, st));
                 QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
                 QG_CUDA_TRY(cudaStreamSynchronize(st));
                 solve_info = (solve_info == 1) ? 1 : 0;  // the one-block solver returns scaled vectors
+                Z = s.Sa2;
+                ldz = k3;
             } else {
-                k_equilibrate<<<2 * n, 128, 0, st>>>(s.Sa, s.Sb, k3, 2 * n, s.Sa2, s.Sb2);
-                QG_SOLVER_TRY(cusolverDnDsygvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                               CUBLAS_FILL_MODE_LOWER, 2 * n, s.Sa2, k3, s.Sb2, k3, s.w_d,
-                                               s.work.as<double>(), s.lwork, s.info_d));
-                QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
-                QG_CUDA_TRY(cudaStreamSynchronize(st));
-                if (solve_info == 0) {
-                    k_rowscale<<<n, 128, 0, st>>>(Z, k3, 2 * n, s.Sb, k3);
-                    QG_CUDA_TRY(cudaMemset2DAsync(Z + 2 * n, (size_t)k3 * sizeof(double), 0,
-                                                  (size_t)n * sizeof(double), (size_t)n, st));
-                }
+                QG_TRY(s.solve_pencil(2 * n, k3, 2 * n, &Z, &ldz, &solve_info));
             }
-        } else if (solve_info == 0) {
-            k_rowscale<<<n, 128, 0, st>>>(Z, k3, k3, s.Sb, k3);  // z = D z'
         }
         if (solve_info != 0) {
             status = solve_info > 0 ? QG_ERR_CHOLESKY : QG_ERR_LIBRARY;
@@ -383,11 +498,11 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
         }
         if (restarted) ++restarts;
         tm.mark(3, st);
-        // rotation: columns 0..n-1 of Z are (Cx; Cr; Cp)
-        QG_TRY(s.gemm_nn(k3 - n, s.r, Z + n, k3, s.Tp));    // p_new = [r p] [Cr; Cp]
-        QG_TRY(s.gemm_nn(k3 - n, s.Ar, Z + n, k3, s.ATp));
-        QG_TRY(s.gemm_nn(k3, s.x, Z, k3, s.Tx));            // x_new = [x r p] [Cx; Cr; Cp]
-        QG_TRY(s.gemm_nn(k3, s.Ax, Z, k3, s.ATx));
+        // rotation: columns 0..n-1 of Z are (Cx; Cr; Cp) (c rows/columns per state)
+        QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp));   // p_new = [r p] [Cr; Cp]
+        QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.Ar, Z + c * n, ldz, s.ATp));
+        QG_TRY(s.gemm_nn(c * k3, c * n, s.x, Z, ldz, s.Tx));                 // x_new = [x r p] [Cx; Cr; Cp]
+        QG_TRY(s.gemm_nn(c * k3, c * n, s.Ax, Z, ldz, s.ATx));
         QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Ax, s.ATx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
@@ -396,7 +511,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, double* ev
         s.normalize(s.x, s.Ax);
         s.normalize(s.p, s.Ap);
         s.coldot(s.x, s.Ax, s.dV, s.ev_d);
-        k_residual<<<n, kRedThreads, 0, st>>>(s.Ax, s.x, s.ev_d, s.r, N, N, s.dV, s.nr_d);
+        s.residual();
         QG_CUDA_TRY(cudaGetLastError());
         QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
         if (pc) {  // next search direction w = T r, normalised (the residual norms are already taken)
@@ -458,13 +573,25 @@ extern "C" {
 int qg_lobpcg_d(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
                 qg_lobpcg_report* rep) {
     if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
-    return run_lobpcg(h, opt, ns, ev, nullptr, nullptr, X, X, P, P, rep);
+    return run_lobpcg(h, opt, ns, 1, ev, nullptr, nullptr, X, X, P, P, rep);
 }
 
 int qg_lobpcg_d_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
                        qg_lobpcg_report* rep) {
     if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
-    return run_lobpcg(h, opt, ns, ev, X, P, nullptr, nullptr, nullptr, nullptr, rep);
+    return run_lobpcg(h, opt, ns, 1, ev, X, P, nullptr, nullptr, nullptr, nullptr, rep);
+}
+
+int qg_lobpcg_z(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
+                qg_lobpcg_report* rep) {
+    if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
+    return run_lobpcg(h, opt, ns, 2, ev, nullptr, nullptr, X, X, P, P, rep);
+}
+
+int qg_lobpcg_z_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
+                       qg_lobpcg_report* rep) {
+    if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
+    return run_lobpcg(h, opt, ns, 2, ev, X, P, nullptr, nullptr, nullptr, nullptr, rep);
 }
 
 }  // extern "C"

@@ -118,6 +118,9 @@ def lib():
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
+        L.qg_lobpcg_z.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
+        L.qg_lobpcg_z_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
+                                         C.POINTER(LobpcgReport)]
         L.qg_lobpcg_d_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
         _lib = L
@@ -269,6 +272,40 @@ class Hamiltonian:
                                C.byref(rep))
         if st not in (QG_OK, -9):
             check(st, "qg_lobpcg_d")
+        return dict(ev=ev, X=X, P=P, report=rep.as_dict(), status=st)
+
+    def lobpcg_device(self, X, P=None, max_iter=2000, tol=1.0e-10, first=True, verbose=False, precond=0,
+                      shift=1.0, complex_states=False):
+        """Block LOBPCG on device tensors (float64 CUDA, (ns, N) real or (ns, 2N)
+        split-complex): X is overwritten with the eigenvectors, P (same shape, may be
+        None on a first call) with the last search directions. Returns dict(ev, report, status)."""
+        assert X.is_cuda and X.dtype.is_floating_point and X.is_contiguous()
+        ns = X.shape[0]
+        ev = np.zeros(ns)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0, precond, shift)
+        rep = LobpcgReport()
+        self.ctx.use_torch_stream()
+        fn = lib().qg_lobpcg_z_device if complex_states else lib().qg_lobpcg_d_device
+        st = fn(self.h, C.byref(opt), ns, ev.ctypes.data_as(_dp), C.c_void_p(X.data_ptr()),
+                C.c_void_p(P.data_ptr() if P is not None else 0), C.byref(rep))
+        if st not in (QG_OK, -9):
+            check(st, "qg_lobpcg_z_device" if complex_states else "qg_lobpcg_d_device")
+        return dict(ev=ev, report=rep.as_dict(), status=st)
+
+    def lobpcg_z(self, X0, max_iter=2000, tol=1.0e-10, P0=None, first=True, verbose=False, precond=0,
+                 shift=1.0):
+        """Complex block LOBPCG (qg_lobpcg_z) for the k-point operator from host
+        split-complex states X0 (ns, 2N); returns dict(ev, X, P, report, status)."""
+        X = np.ascontiguousarray(X0, dtype=np.float64).copy()
+        ns = X.shape[0]
+        P = np.zeros_like(X) if P0 is None else np.ascontiguousarray(P0, dtype=np.float64).copy()
+        ev = np.zeros(ns)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0, precond, shift)
+        rep = LobpcgReport()
+        st = lib().qg_lobpcg_z(self.h, C.byref(opt), ns, ev.ctypes.data_as(_dp), X.ctypes.data, P.ctypes.data,
+                               C.byref(rep))
+        if st not in (QG_OK, -9):
+            check(st, "qg_lobpcg_z")
         return dict(ev=ev, X=X, P=P, report=rep.as_dict(), status=st)
 
     def apply_timed(self, ns, x_ptr, hx_ptr):

@@ -153,3 +153,12 @@ def test_port_kpoint_matches_live_reference_on_fresh_cell():
     a = O.hamiltonian_kpoint_apply(cell, g, X, impl="port")
     b = O.hamiltonian_kpoint_apply(cell, g, X, impl="ref")
     assert rel(a, b) < 1e-14
+
+
+def test_port_dense_kpoint_spectrum_matches_reference_complex_solver():
+    # eigenvalues of the port's k-point operator (dense) against the reference's
+    # own Eigen_z_multi_mpi run on the reference operator (golden fixture)
+    g = np.load(os.path.join(GOLD, "lobpcg_kpoint.npz"))
+    cell = build_cell(grid=(12, 12, 12), a0=4.4)
+    w = np.linalg.eigvalsh(O.dense_kpoint_hamiltonian(cell, tuple(g["small_g"])))
+    np.testing.assert_allclose(w[:6], np.sort(g["small_ev"]), rtol=0, atol=1e-10)
