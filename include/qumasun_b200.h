@@ -180,6 +180,8 @@ typedef struct qg_lobpcg_options {
     int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
                            applied in Fourier space with the FD stencil's own symbol */
     double precond_shift; /* shift (Ha) of the kinetic preconditioner; <= 0 selects 1.0 */
+    int n_converge;     /* the lowest n_converge states must meet tol, the others are a guard
+                           band against a degenerate multiplet at the cut; <= 0 or >= ns: all */
 } qg_lobpcg_options;
 
 typedef struct qg_lobpcg_report {
@@ -188,8 +190,9 @@ typedef struct qg_lobpcg_report {
     double max_residual;/* max_j sum_i r_j(i)^2 dV at exit */
     double ms_total;    /* device time of the solve */
     double ms_hamiltonian, ms_gram, ms_eigensolve, ms_rotate, ms_vector;  /* per-phase device time */
-    int restarts;       /* iterations whose [x r p] Gram matrix was singular and that
-                           continued from [x r] alone (P dropped) */
+    int restarts;       /* iterations whose [x r p] Gram matrix was not positive definite at
+                           working precision and that were solved on its numerically
+                           nonsingular subspace (eigenvalues of B above 1e-12 max) */
 } qg_lobpcg_report;
 
 /* Block LOBPCG for the ns lowest eigenpairs of H, FP64 on the GPU.
@@ -203,11 +206,11 @@ typedef struct qg_lobpcg_report {
  * w_dsygvx.h:24-104). X (ns*N, in/out), P (ns*N, in/out, the reference's
  * "keep") and ev (ns, out) are HOST buffers, state-major. The pencil is
  * Jacobi-equilibrated (scaled to unit diag(B)) and solved with cuSOLVER's
- * sygvd; if B is still not positive definite the step continues from [x r]
- * alone (P dropped, counted in report->restarts; pencils of up to 80 rows then
- * go to the library's own one-block Jacobi solver). Returns
- * QG_ERR_NOT_CONVERGED (results still written) when max_iter is reached,
- * QG_ERR_CHOLESKY if the Gram matrix of [x r p] is not positive definite. */
+ * sygvd; if B is still not positive definite, the step is solved on the span
+ * of B's eigenvectors with eigenvalues above 1e-12 max (counted in
+ * report->restarts) instead of stopping. Returns QG_ERR_NOT_CONVERGED (results
+ * still written) when max_iter is reached, QG_ERR_CHOLESKY if fewer than ns
+ * independent directions remain. */
 int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
                 double* P, qg_lobpcg_report* report);
 /* Same with DEVICE buffers X and P (ld = N); ev stays a host array. */

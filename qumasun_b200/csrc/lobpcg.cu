@@ -210,6 +210,31 @@ __global__ void k_expand_rotation(const cuDoubleComplex* __restrict__ Z, int ldz
     }
 }
 
+// Fills the upper triangle of the leading k x k block from the lower one
+// (conjugated for complex entries); one block per column j.
+template <typename T>
+__global__ void k_mirror_lower(T* __restrict__ A, int ld, int k) {
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+        const T v = A[j + (long long)i * ld];
+        if constexpr (sizeof(T) == 16) A[i + (long long)j * ld] = cuConj(v);
+        else A[i + (long long)j * ld] = v;
+    }
+}
+
+// T(:, j) = V(:, f + j) / sqrt(s[f + j]) for the kp eigenvectors of B kept.
+template <typename T>
+__global__ void k_scaled_basis(const T* __restrict__ V, int ld, int k, const double* __restrict__ s, int f,
+                               T* __restrict__ Tm) {
+    const int j = blockIdx.x;
+    const double sc = 1.0 / sqrt(s[f + j]);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const T v = V[i + (long long)(f + j) * ld];
+        if constexpr (sizeof(T) == 16) Tm[i + (long long)j * ld] = make_cuDoubleComplex(cuCreal(v) * sc, cuCimag(v) * sc);
+        else Tm[i + (long long)j * ld] = v * sc;
+    }
+}
+
 struct Timer {
     cudaEvent_t ev[8];
     int n = 0;
@@ -251,15 +276,18 @@ struct Solver {
     cudaStream_t st;
     cublasHandle_t blas;
     cusolverDnHandle_t sol;
-    DevBuf W, AW, T, AT, S, small, work;
+    DevBuf W, AW, T, AT, S, E, small, work;
     int lwork = 0;
     double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb, *Sa2, *Sb2, *M;
+    double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
+    std::vector<double> s_h;
     cuDoubleComplex *Ca, *Cb;
     double *ev_d, *nr_d, *f_d, *f2_d, *w_d;
     int* info_d;
 
     ~Solver() {
-        W.release(); AW.release(); T.release(); AT.release(); S.release(); small.release(); work.release();
+        W.release(); AW.release(); T.release(); AT.release(); S.release(); E.release(); small.release();
+        work.release();
     }
 
     int setup() {
@@ -273,6 +301,9 @@ struct Solver {
         // for c = 2 the real rotation matrix (2 k3 x 2 n)
         QG_TRY(S.reserve((2 * g3 * g3 + 2 * c * k3 * k3 + (c == 2 ? g3 * 2 * n : 0)) * sizeof(double)));
         QG_TRY(small.reserve((5 * k3 + 16) * sizeof(double)));
+        QG_TRY(E.reserve(4 * (size_t)c * k3 * k3 * sizeof(double)));
+        E0 = E.as<double>();
+        s_h.resize(k3);
         x = W.as<double>(); r = x + blk; p = r + blk;
         Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
         Tx = T.as<double>(); Tp = Tx + blk;
@@ -289,11 +320,19 @@ struct Solver {
             QG_SOLVER_TRY(cusolverDnDsygvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
                                                       CUBLAS_FILL_MODE_LOWER, (int)k3, Sa2, (int)k3, Sb2, (int)k3,
                                                       w_d, &lwork));
+            int lw2 = 0;
+            QG_SOLVER_TRY(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)k3,
+                                                      Sb2, (int)k3, w_d, &lw2));
+            lwork = std::max(lwork, lw2);
             QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(double)));
         } else {
             QG_SOLVER_TRY(cusolverDnZhegvd_bufferSize(sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
                                                       CUBLAS_FILL_MODE_LOWER, (int)k3, Ca, (int)k3, Cb, (int)k3,
                                                       w_d, &lwork));
+            int lw2 = 0;
+            QG_SOLVER_TRY(cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)k3,
+                                                      Cb, (int)k3, w_d, &lw2));
+            lwork = std::max(lwork, lw2);
             QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(cuDoubleComplex)));
         }
         QG_TRY(h->coef.reserve((size_t)c * qg::coef_scratch_elems(h, n) * sizeof(double)));
@@ -388,6 +427,80 @@ struct Solver {
         }
         return QG_OK;
     }
+
+    // Fallback when B of the pencil is not positive definite at working precision:
+    // solve on B's numerically nonsingular subspace instead of dropping P.
+    //   B2 = V diag(s) V^T (eigendecomposition), keep s_i > 1e-12 max(s),
+    //   T = V_kept diag(s_kept)^-1/2,  (T^T A2 T) y = lambda y,  z' = T y,  z = D z'
+    // (A2, B2 the Jacobi-equilibrated pencil, D its scaling). Leaves the rotation
+    // matrix like solve_pencil. Returns QG_ERR_CHOLESKY if fewer than n directions survive.
+    int solve_truncated(int k, int k3, const double** Zout, int* ldz) {
+        int info = 0;
+        const size_t kk = (size_t)k3 * k3;
+        if (c == 1) {
+            double* Tm = E0;
+            double* tmp = Tm + kk;
+            double* Ar = tmp + kk;
+            double* Zt = Ar + kk;
+            k_equilibrate<<<k, 128, 0, st>>>(Sa, Sb, k3, k, Sa2, Sb2);
+            k_mirror_lower<double><<<k, 128, 0, st>>>(Sa2, k3, k);
+            QG_SOLVER_TRY(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, Sb2, k3, w_d,
+                                           work.as<double>(), lwork, info_d));
+            QG_TRY(read_spectrum(k, &info));
+            if (info != 0) return QG_ERR_LIBRARY;
+            int f = 0;
+            const double thr = 1e-12 * s_h[k - 1];
+            while (f < k && !(s_h[f] > thr)) ++f;
+            const int kp = k - f;
+            if (kp < n) return QG_ERR_CHOLESKY;
+            k_scaled_basis<double><<<kp, 128, 0, st>>>(Sb2, k3, k, w_d, f, Tm);
+            const double one = 1.0, zero = 0.0;
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kp, k, &one, Sa2, k3, Tm, k3, &zero, tmp, k3));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, kp, kp, k, &one, Tm, k3, tmp, k3, &zero, Ar, k3));
+            QG_SOLVER_TRY(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, kp, Ar, k3, w_d,
+                                           work.as<double>(), lwork, info_d));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k, n, kp, &one, Tm, k3, Ar, k3, &zero, Zt, k3));
+            k_rowscale<<<n, 128, 0, st>>>(Zt, k3, k, Sb, k3);  // z = D z'
+            *Zout = Zt;
+            *ldz = k3;
+        } else {
+            cuDoubleComplex* Tm = reinterpret_cast<cuDoubleComplex*>(E0);
+            cuDoubleComplex* tmp = Tm + kk;
+            cuDoubleComplex* Ar = tmp + kk;
+            cuDoubleComplex* Zt = Ar + kk;
+            k_gram_to_complex<<<k, 128, 0, st>>>(Sa, Sb, 2 * k3, k, Ca, Cb, k3);
+            k_mirror_lower<cuDoubleComplex><<<k, 128, 0, st>>>(Ca, k3, k);
+            QG_SOLVER_TRY(cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k, Cb, k3, w_d,
+                                           work.as<cuDoubleComplex>(), lwork, info_d));
+            QG_TRY(read_spectrum(k, &info));
+            if (info != 0) return QG_ERR_LIBRARY;
+            int f = 0;
+            const double thr = 1e-12 * s_h[k - 1];
+            while (f < k && !(s_h[f] > thr)) ++f;
+            const int kp = k - f;
+            if (kp < n) return QG_ERR_CHOLESKY;
+            k_scaled_basis<cuDoubleComplex><<<kp, 128, 0, st>>>(Cb, k3, k, w_d, f, Tm);
+            const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+            QG_BLAS_TRY(cublasZgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k, kp, k, &one, Ca, k3, Tm, k3, &zero, tmp, k3));
+            QG_BLAS_TRY(cublasZgemm(blas, CUBLAS_OP_C, CUBLAS_OP_N, kp, kp, k, &one, Tm, k3, tmp, k3, &zero, Ar, k3));
+            QG_SOLVER_TRY(cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, kp, Ar, k3, w_d,
+                                           work.as<cuDoubleComplex>(), lwork, info_d));
+            QG_BLAS_TRY(cublasZgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k, n, kp, &one, Tm, k3, Ar, k3, &zero, Zt, k3));
+            k_expand_rotation<<<n, 128, 0, st>>>(Zt, k3, k3, k, Sb, 2 * k3, M, 2 * k3);
+            *Zout = M;
+            *ldz = 2 * k3;
+        }
+        QG_CUDA_TRY(cudaGetLastError());
+        return QG_OK;
+    }
+
+    // eigenvalues of B (w_d, ascending) and the solver info to the host
+    int read_spectrum(int k, int* info) {
+        QG_CUDA_TRY(cudaMemcpyAsync(s_h.data(), w_d, k * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(info, info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        return QG_OK;
+    }
 };
 
 int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps, double* ev, double* X_dev,
@@ -462,6 +575,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     int status = QG_OK;
     int restarts = 0;
     const int c = comps;
+    const int nconv = (opt->n_converge > 0 && opt->n_converge < n) ? opt->n_converge : n;
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
@@ -472,24 +586,18 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         tm.mark(2, st);
         // Jacobi-equilibrated pencil (keeps the tiny residual columns of the reference
         // iteration from ruining the Cholesky factor of B), cuSOLVER sygvd / hegvd on it;
-        // if B is still not positive definite, restart this step without P
+        // if B is still not positive definite, the step is solved on B's numerically
+        // nonsingular subspace (counted as a restart)
         const double* Z = nullptr;
         int ldz = 0;
         bool restarted = false;
         int solve_info = 0;
         QG_TRY(s.solve_pencil(k3, k3, k3, &Z, &ldz, &solve_info));
-        if (solve_info > 0 && k3 == 3 * n) {
+        if (solve_info > 0) {
             restarted = true;
-            if (c == 1 && k3 <= qg::kSmallEigMax) {
-                QG_TRY(qg::small_eig_launch(s.Sa, s.Sb, k3, 0, k3, 2 * n, s.Sa2, k3, 0, s.w_d, 0, s.info_d, 1, st));
-                QG_CUDA_TRY(cudaMemcpyAsync(&solve_info, s.info_d, sizeof(int), cudaMemcpyDeviceToHost, st));
-                QG_CUDA_TRY(cudaStreamSynchronize(st));
-                solve_info = (solve_info == 1) ? 1 : 0;  // the one-block solver returns scaled vectors
-                Z = s.Sa2;
-                ldz = k3;
-            } else {
-                QG_TRY(s.solve_pencil(2 * n, k3, 2 * n, &Z, &ldz, &solve_info));
-            }
+            const int rc = s.solve_truncated(k3, k3, &Z, &ldz);
+            if (rc == QG_OK) solve_info = 0;
+            else if (rc != QG_ERR_CHOLESKY) solve_info = -1;
         }
         if (solve_info != 0) {
             status = solve_info > 0 ? QG_ERR_CHOLESKY : QG_ERR_LIBRARY;
@@ -522,7 +630,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         tm.mark(-1, st);
         QG_CUDA_TRY(cudaStreamSynchronize(st));
         tm.flush();
-        maxres = *std::max_element(nr_h.begin(), nr_h.end());
+        maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
         if (!std::isfinite(maxres)) {
             status = QG_ERR_NONFINITE;
             ++it;

@@ -65,7 +65,7 @@ class LobpcgOptions(C.Structure):
 
     _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("first_call", C.c_int),
                 ("precision", C.c_int), ("verbose", C.c_int), ("precond", C.c_int),
-                ("precond_shift", C.c_double)]
+                ("precond_shift", C.c_double), ("n_converge", C.c_int)]
 
 
 class LobpcgReport(C.Structure):
@@ -275,14 +275,15 @@ class Hamiltonian:
         return dict(ev=ev, X=X, P=P, report=rep.as_dict(), status=st)
 
     def lobpcg_device(self, X, P=None, max_iter=2000, tol=1.0e-10, first=True, verbose=False, precond=0,
-                      shift=1.0, complex_states=False):
+                      shift=1.0, complex_states=False, n_converge=0, precision=0):
         """Block LOBPCG on device tensors (float64 CUDA, (ns, N) real or (ns, 2N)
         split-complex): X is overwritten with the eigenvectors, P (same shape, may be
         None on a first call) with the last search directions. Returns dict(ev, report, status)."""
         assert X.is_cuda and X.dtype.is_floating_point and X.is_contiguous()
         ns = X.shape[0]
         ev = np.zeros(ns)
-        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0, precond, shift)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, precision, 1 if verbose else 0, precond, shift,
+                            n_converge)
         rep = LobpcgReport()
         self.ctx.use_torch_stream()
         fn = lib().qg_lobpcg_z_device if complex_states else lib().qg_lobpcg_d_device
