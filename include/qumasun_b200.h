@@ -37,7 +37,11 @@ typedef enum qg_status {
     QG_ERR_NOT_CONVERGED = -9  /* solver hit its iteration limit (results still written) */
 } qg_status;
 
-typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1 } qg_precision;
+/* QG_MIXED_BF16X3 (LOBPCG only): the Gram products run as split-BF16x3 tensor-core
+ * GEMMs with FP32 accumulation (FP64 across K chunks); H, residuals, rotations,
+ * norms and the small eigensolves stay FP64, and a final FP64 Rayleigh-Ritz on X
+ * sets the returned eigenpairs. */
+typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2 } qg_precision;
 
 typedef struct qg_context_s* qg_context;
 typedef struct qg_hamiltonian_s* qg_hamiltonian;
@@ -175,7 +179,7 @@ typedef struct qg_lobpcg_options {
     double tol;         /* stop when max_j sum_i r_j(i)^2 dV < tol * dV (reference limit 1e-10,
                            lobpcg_d_multi.h:54, :525); <= 0 selects 1e-10 */
     int first_call;     /* 1: start with P = 0 and the 2n x 2n first step (reference is_first_time) */
-    int precision;      /* QG_FP64: FP64 throughout */
+    int precision;      /* QG_FP64: FP64 throughout; QG_MIXED_BF16X3: split-BF16x3 Gram products */
     int verbose;        /* 1: print (iteration, max residual) lines to stdout */
     int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
                            applied in Fourier space with the FD stencil's own symbol */

@@ -1,0 +1,111 @@
+// Mixed-precision Gram products for LOBPCG: S = alpha A^T B with A, B tall
+// N x m FP64 blocks (ld N), computed as split-BF16x3 with FP32 accumulation:
+//   a = a_hi + a_lo,  a_hi = bf16(a),  a_lo = bf16(a - a_hi)   (same for b)
+//   a.b ~ a_hi.b_hi + a_hi.b_lo + a_lo.b_hi                      (a_lo.b_lo dropped, ~2^-17 relative)
+// The K (grid) dimension is cut into chunks of kChunk rows; every chunk is an
+// FP32-accumulated tensor-core product, the chunk partials are summed in FP64 in a
+// fixed order (deterministic), so the FP32 error grows with the chunk length only.
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "gram_mixed.h"
+
+namespace qg {
+namespace {
+
+__global__ void k_split_bf16(const double* __restrict__ src, long long n, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double v = src[i];
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        hi[i] = h;
+        lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
+    }
+}
+
+// C[e] = alpha * sum_c P[c][e] for e < m*m, chunks in order.
+__global__ void k_reduce_chunks(const float* __restrict__ P, int nchunk, long long mm, double alpha,
+                                double* __restrict__ C) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < mm; e += stride) {
+        double s = 0.0;
+        for (int c = 0; c < nchunk; ++c) s += (double)P[(long long)c * mm + e];
+        C[e] = alpha * s;
+    }
+}
+
+#define QG_MG_BLAS_TRY(expr)                                           \
+    do {                                                               \
+        cublasStatus_t qg_b_ = (expr);                                 \
+        if (qg_b_ != CUBLAS_STATUS_SUCCESS) {                          \
+            qg_set_last_error(#expr, "cublas error", __FILE__, __LINE__); \
+            return QG_ERR_LIBRARY;                                     \
+        }                                                              \
+    } while (0)
+
+}  // namespace
+
+int MixedGram::setup(long long N_, int mmax_) {
+    N = N_;
+    mmax = mmax_;
+    const size_t elems = (size_t)N * mmax;
+    QG_TRY(split_a.reserve(2 * elems * sizeof(__nv_bfloat16)));
+    QG_TRY(split_b.reserve(2 * elems * sizeof(__nv_bfloat16)));
+    nfull = (int)(N / kChunk);
+    rem = (int)(N - (long long)nfull * kChunk);
+    const int nparts = nfull + (rem ? 1 : 0);
+    QG_TRY(part.reserve((size_t)nparts * mmax * mmax * sizeof(float)));
+    return QG_OK;
+}
+
+int MixedGram::split(const double* A, int m, int which, cudaStream_t st) {
+    const long long n = N * m;
+    DevBuf& b = which == 0 ? split_a : split_b;
+    __nv_bfloat16* hi = b.as<__nv_bfloat16>();
+    __nv_bfloat16* lo = hi + (size_t)N * mmax;
+    k_split_bf16<<<148 * 8, 256, 0, st>>>(A, n, hi, lo);
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
+
+int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, double alpha, double* C, int ldc) {
+    const __nv_bfloat16* ahi = split_a.as<__nv_bfloat16>();
+    const __nv_bfloat16* alo = ahi + (size_t)N * mmax;
+    const __nv_bfloat16* bhi = b_is_a ? ahi : split_b.as<__nv_bfloat16>();
+    const __nv_bfloat16* blo = bhi + (size_t)N * mmax;
+    float* P = part.as<float>();
+    const long long mm = (long long)m * m;
+    const float one = 1.0f, zero = 0.0f;
+    const __nv_bfloat16* As[3] = {ahi, ahi, alo};
+    const __nv_bfloat16* Bs[3] = {bhi, blo, bhi};
+    QG_MG_BLAS_TRY(cublasSetStream(blas, st));
+    for (int t = 0; t < 3; ++t) {
+        const float* beta = t == 0 ? &zero : &one;
+        if (nfull > 0)
+            QG_MG_BLAS_TRY(cublasGemmStridedBatchedEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, kChunk, &one, As[t],
+                                                      CUDA_R_16BF, (int)N, kChunk, Bs[t], CUDA_R_16BF, (int)N, kChunk,
+                                                      beta, P, CUDA_R_32F, m, mm, nfull, CUBLAS_COMPUTE_32F,
+                                                      CUBLAS_GEMM_DEFAULT));
+        if (rem)
+            QG_MG_BLAS_TRY(cublasGemmEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, rem, &one,
+                                        As[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N,
+                                        Bs[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N, beta,
+                                        P + (long long)nfull * mm, CUDA_R_32F, m, CUBLAS_COMPUTE_32F,
+                                        CUBLAS_GEMM_DEFAULT));
+    }
+    if (ldc != m) return QG_ERR_INVALID;
+    k_reduce_chunks<<<148 * 4, 256, 0, st>>>(P, nfull + (rem ? 1 : 0), mm, alpha, C);
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
+
+void MixedGram::release() {
+    split_a.release();
+    split_b.release();
+    part.release();
+}
+
+}  // namespace qg

@@ -1,19 +1,23 @@
-// Block LOBPCG on the GPU, FP64 (EigenLOBPCG_d_multi, lobpcg_d_multi.h:23-545).
+// Block LOBPCG on the GPU, FP64 (EigenLOBPCG_d_multi, lobpcg_d_multi.h:23-545;
+// complex states: Eigen_z_multi_mpi, lobpcg_z_multi_mpi.h:988-1800).
 //
 // Blocks live on the device as column-major N x n arrays (= the reference's
-// state-major layout, one state per column):
+// state-major layout, one state per column; a split-complex state is two
+// consecutive columns {re, im}):
 //   W  = [x | r | p]      (3n columns, contiguous)
 //   AW = [Ax | Ar | Ap]
-//   T  = [x_new | p_new], AT = [Ax_new | Ap_new] (rotation outputs)
+//   T  = [x_new | p_new]  (rotation outputs)
 // One iteration:
-//   Ar = H r                                       (qg::apply_hamiltonian)
-//   Sa = W^T AW dV, Sb = W^T W dV                  (DGEMM; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
+//   Ar = H r                                       (qg::apply_hamiltonian / _z)
+//   Sa = W^T AW dV, Sb = W^T W dV                  (DSYRKX / DSYRK, lower triangles; DGEMM for
+//                                                   complex; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
 //   Sa z = lambda Sb z, k = 3n (2n on the first step of a first call), Jacobi-equilibrated,
-//   cusolverDnDsygvd (replaces DSYGVX, w_dsygvx.h:24-104, UPLO as the reference); a
-//   singular [x r p] Gram matrix restarts the step from [x r] (P coefficients zero)
-//   p_new = [r p] [Cr; Cp], x_new = [x r p] [Cx; Cr; Cp] (DGEMM; lobpcg_d_multi.h:247-300)
-//   renormalise x, Ax by |x|, p, Ap by |p| (:491-505); ei = x.Ax dV; r = Ax - ei x (:506-512)
-//   stop when max_j sum r_j^2 dV < tol dV (:525).
+//   cusolverDnDsygvd / Zhegvd (replaces DSYGVX / ZHEGVX, w_dsygvx.h:24-104, UPLO as the
+//   reference); if B is not positive definite the step is solved on B's nonsingular subspace
+//   p_new = [r p] [Cr; Cp], x_new = x Cx + p_new   (DGEMM; lobpcg_d_multi.h:247-300)
+//   renormalise x and p (:491-505); Ax = H x_new, Ap = H p_new (re-applied, not rotated);
+//   ei = x.Ax dV; r = Ax - ei x (:506-512)
+//   stop when max_j sum r_j^2 dV < tol dV over the lowest n_converge states (:525).
 // Column reductions (norms, dots, residuals) are project kernels with one
 // block per column and a fixed reduction order (deterministic).
 #include <cublas_v2.h>
@@ -25,6 +29,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "gram_mixed.h"
 #include "precond.h"
 #include "qg_internal.h"
 #include "small_eig.h"
@@ -236,10 +241,10 @@ __global__ void k_scaled_basis(const T* __restrict__ V, int ld, int k, const dou
 }
 
 struct Timer {
-    cudaEvent_t ev[8];
+    cudaEvent_t ev[16];
     int n = 0;
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    int tag[8];
+    int tag[16];
     bool ok = true;
     Timer() {
         for (auto& e : ev)
@@ -249,7 +254,7 @@ struct Timer {
         for (auto e : ev) cudaEventDestroy(e);
     }
     void mark(int t, cudaStream_t st) {
-        if (n < 8) {
+        if (n < 16) {
             cudaEventRecord(ev[n], st);
             tag[n++] = t;
         }
@@ -276,17 +281,20 @@ struct Solver {
     cudaStream_t st;
     cublasHandle_t blas;
     cusolverDnHandle_t sol;
-    DevBuf W, AW, T, AT, S, E, small, work;
+    DevBuf W, AW, T, S, E, small, work;
     int lwork = 0;
-    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *ATx, *ATp, *Sa, *Sb, *Sa2, *Sb2, *M;
+    double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *Sa, *Sb, *Sa2, *Sb2, *M;
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
     std::vector<double> s_h;
+    bool mixed = false;      // split-BF16x3 Gram products (qg::MixedGram)
+    double trunc_eps = 1e-12;  // relative eigenvalue floor of B in the rank-revealing solve
+    qg::MixedGram mg;
     cuDoubleComplex *Ca, *Cb;
     double *ev_d, *nr_d, *f_d, *f2_d, *w_d;
     int* info_d;
 
     ~Solver() {
-        W.release(); AW.release(); T.release(); AT.release(); S.release(); E.release(); small.release();
+        W.release(); AW.release(); T.release(); S.release(); E.release(); small.release();
         work.release();
     }
 
@@ -295,7 +303,6 @@ struct Solver {
         QG_TRY(W.reserve(3 * blk * sizeof(double)));
         QG_TRY(AW.reserve(3 * blk * sizeof(double)));
         QG_TRY(T.reserve(2 * blk * sizeof(double)));
-        QG_TRY(AT.reserve(2 * blk * sizeof(double)));
         const size_t k3 = 3 * (size_t)n, g3 = c * k3;
         // real Gram pair (c k3)^2 each; the equilibrated pencil (k3^2 real or complex each);
         // for c = 2 the real rotation matrix (2 k3 x 2 n)
@@ -307,7 +314,6 @@ struct Solver {
         x = W.as<double>(); r = x + blk; p = r + blk;
         Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
         Tx = T.as<double>(); Tp = Tx + blk;
-        ATx = AT.as<double>(); ATp = ATx + blk;
         Sa = S.as<double>(); Sb = Sa + g3 * g3; Sa2 = Sb + g3 * g3; Sb2 = Sa2 + c * k3 * k3;
         M = Sb2 + c * k3 * k3;
         // the triangle DSYRK(X) leaves unwritten stays finite (zero)
@@ -336,6 +342,7 @@ struct Solver {
             QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(cuDoubleComplex)));
         }
         QG_TRY(h->coef.reserve((size_t)c * qg::coef_scratch_elems(h, n) * sizeof(double)));
+        if (mixed) QG_TRY(mg.setup(N, (int)g3));
         return QG_OK;
     }
 
@@ -377,6 +384,13 @@ struct Solver {
     // (DSYRKX / DSYRK, half the flops; the eigensolvers read the lower triangle);
     // the split-complex Gram is not symmetric column by column, so it takes full DGEMMs.
     int gram(int m) {
+        if (mixed) {
+            QG_TRY(mg.split(x, m, 0, st));
+            QG_TRY(mg.split(Ax, m, 1, st));
+            QG_TRY(mg.gram(blas, st, m, false, dV, Sa, m));
+            QG_TRY(mg.gram(blas, st, m, true, dV, Sb, m));
+            return QG_OK;
+        }
         if (c == 2) {
             QG_TRY(gemm_tn(m, m, x, Ax, dV, Sa, m));
             return gemm_tn(m, m, x, x, dV, Sb, m);
@@ -388,10 +402,10 @@ struct Solver {
         return QG_OK;
     }
 
-    // C (N x nc) = A (N x k) * Z (k x nc, ldz)
-    int gemm_nn(int k, int nc, const double* A, const double* Z, int ldz, double* C) {
-        const double one = 1.0, zero = 0.0;
-        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nc, k, &one, A, (int)N, Z, ldz, &zero, C,
+    // C (N x nc) = A (N x k) * Z (k x nc, ldz) + beta C
+    int gemm_nn(int k, int nc, const double* A, const double* Z, int ldz, double* C, double beta) {
+        const double one = 1.0;
+        QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nc, k, &one, A, (int)N, Z, ldz, &beta, C,
                                 (int)N));
         return QG_OK;
     }
@@ -449,7 +463,7 @@ struct Solver {
             QG_TRY(read_spectrum(k, &info));
             if (info != 0) return QG_ERR_LIBRARY;
             int f = 0;
-            const double thr = 1e-12 * s_h[k - 1];
+            const double thr = trunc_eps * s_h[k - 1];
             while (f < k && !(s_h[f] > thr)) ++f;
             const int kp = k - f;
             if (kp < n) return QG_ERR_CHOLESKY;
@@ -475,7 +489,7 @@ struct Solver {
             QG_TRY(read_spectrum(k, &info));
             if (info != 0) return QG_ERR_LIBRARY;
             int f = 0;
-            const double thr = 1e-12 * s_h[k - 1];
+            const double thr = trunc_eps * s_h[k - 1];
             while (f < k && !(s_h[f] > thr)) ++f;
             const int kp = k - f;
             if (kp < n) return QG_ERR_CHOLESKY;
@@ -509,7 +523,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
     if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
     if (comps == 2 && h->order != 8) return QG_ERR_UNSUPPORTED;
-    if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
+    if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3) return QG_ERR_UNSUPPORTED;
     if (opt->precond != 0 && opt->precond != 1) return QG_ERR_INVALID;
     const long long N = h->N();
     if ((long long)n * 3 > N) return QG_ERR_INVALID;
@@ -522,6 +536,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     s.L = comps * N;
     s.dV = h->hx * h->hy * h->hz;
     s.st = h->ctx->stream;
+    s.mixed = opt->precision == QG_MIXED_BF16X3;
+    s.trunc_eps = s.mixed ? 1e-6 : 1e-12;
     QG_TRY(qg_blas_handle(h->ctx, &s.blas));
     QG_TRY(qg_solver_handle(h->ctx, &s.sol));
     QG_TRY(s.setup());
@@ -592,7 +608,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         int ldz = 0;
         bool restarted = false;
         int solve_info = 0;
-        QG_TRY(s.solve_pencil(k3, k3, k3, &Z, &ldz, &solve_info));
+        if (s.mixed) solve_info = 1;  // the BF16x3 pencil always takes the rank-revealing solve
+        else QG_TRY(s.solve_pencil(k3, k3, k3, &Z, &ldz, &solve_info));
         if (solve_info > 0) {
             restarted = true;
             const int rc = s.solve_truncated(k3, k3, &Z, &ldz);
@@ -604,20 +621,25 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             ++it;
             break;
         }
-        if (restarted) ++restarts;
+        if (restarted && !s.mixed) ++restarts;
         tm.mark(3, st);
         // rotation: columns 0..n-1 of Z are (Cx; Cr; Cp) (c rows/columns per state)
-        QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp));   // p_new = [r p] [Cr; Cp]
-        QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.Ar, Z + c * n, ldz, s.ATp));
-        QG_TRY(s.gemm_nn(c * k3, c * n, s.x, Z, ldz, s.Tx));                 // x_new = [x r p] [Cx; Cr; Cp]
-        QG_TRY(s.gemm_nn(c * k3, c * n, s.Ax, Z, ldz, s.ATx));
+        //   p_new = [r p] [Cr; Cp],  x_new = x Cx + p_new   (lobpcg_d_multi.h:247-300)
+        // and the A-side blocks are re-applied, Ax = H x_new, Ap = H p_new, instead of
+        // rotated: two memory-bound H applications cost less than the two tall DGEMMs
+        // and keep Ax consistent with x for the residual.
+        QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp, 0.0));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_TRY(s.gemm_nn(c * n, c * n, s.x, Z, ldz, s.Tx, 1.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
-        QG_CUDA_TRY(cudaMemcpyAsync(s.Ax, s.ATx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
-        QG_CUDA_TRY(cudaMemcpyAsync(s.Ap, s.ATp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         tm.mark(4, st);
-        s.normalize(s.x, s.Ax);
-        s.normalize(s.p, s.Ap);
+        s.normalize(s.x, nullptr);
+        s.normalize(s.p, nullptr);
+        tm.mark(0, st);
+        QG_TRY(s.applyH(s.x, s.Ax));
+        QG_TRY(s.applyH(s.p, s.Ap));
+        tm.mark(4, st);
         s.coldot(s.x, s.Ax, s.dV, s.ev_d);
         s.residual();
         QG_CUDA_TRY(cudaGetLastError());
@@ -641,6 +663,30 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             converged = true;
             ++it;
             break;
+        }
+    }
+    // mixed precision: a final FP64 Rayleigh-Ritz on X alone (FP64 Gram of [x], sygvd,
+    // FP64 rotation, Ax re-applied, residual) fixes the eigenvalues to FP64 accuracy
+    if (s.mixed && status == QG_OK) {
+        s.mixed = false;
+        s.trunc_eps = 1e-12;
+        QG_TRY(s.gram(c * n));
+        const double* Z = nullptr;
+        int ldz = 0, info = 0;
+        QG_TRY(s.solve_pencil(n, n, n, &Z, &ldz, &info));
+        if (info > 0) QG_TRY(s.solve_truncated(n, n, &Z, &ldz));
+        else if (info < 0) status = QG_ERR_LIBRARY;
+        if (status == QG_OK) {
+            QG_TRY(s.gemm_nn(c * n, c * n, s.x, Z, ldz, s.Tx, 0.0));
+            QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
+            s.normalize(s.x, nullptr);
+            QG_TRY(s.applyH(s.x, s.Ax));
+            s.coldot(s.x, s.Ax, s.dV, s.ev_d);
+            s.residual();
+            QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            QG_CUDA_TRY(cudaStreamSynchronize(st));
+            maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
+            converged = maxres < tol * s.dV;
         }
     }
     // outputs
