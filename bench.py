@@ -47,7 +47,9 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--sweep", action="store_true", help="also time FD orders 2/4/6 and FP32")
-    p.add_argument("--no-lobpcg", action="store_true", help="skip the LOBPCG time-to-solution leg")
+    p.add_argument("--no-lobpcg", action="store_true", help="skip the LOBPCG time-to-solution legs")
+    p.add_argument("--no-lobpcg216", action="store_true",
+                   help="skip the 216-atom 120^3 LOBPCG leg (FP64 vs BF16x3 Gram, about a minute)")
     p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     return p.parse_args()
@@ -273,6 +275,46 @@ def lobpcg_diamond8(ctx, cpu=True):
     return out
 
 
+def lobpcg_diamond216(ctx):
+    """Time to the 480 lowest eigenpairs (528 solved, a 48-state guard band) of the
+    216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
+    kinetic-preconditioned GPU LOBPCG from the same seeded uniform(-0.5, 0.5) states:
+    FP64 Gram products against split-BF16x3 Gram products (QG_MIXED_BF16X3), which must
+    agree on the 480 eigenvalues to 1e-8 Ha."""
+    import numpy as np
+    import torch
+    from qumasun_b200 import Hamiltonian
+    from qumasun_b200.cell import build_cell
+    cell = build_cell(reps=(3, 3, 3), displacement=0.05, seed=2024)
+    ns, nconv = 528, 480
+    H = Hamiltonian(ctx, cell)
+    gen = torch.Generator(device="cuda").manual_seed(2024)
+    X0 = torch.rand(ns, cell.N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    runs = {}
+    evs = {}
+    for name, prec in (("fp64", 0), ("bf16x3_gram", 2)):
+        X = X0.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = H.lobpcg_device(X, None, max_iter=300, precond=1, shift=1.0, n_converge=nconv, precision=prec)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        rep = r["report"]
+        evs[name] = r["ev"][:nconv]
+        runs[name] = {"seconds": round(wall, 3), "device_ms": round(rep["ms_total"], 1),
+                      "iterations": rep["iterations"], "converged": bool(rep["converged"]),
+                      "mixed_iterations": rep["mixed_iterations"], "restarts": rep["restarts"],
+                      "max_residual": rep["max_residual"],
+                      "phase_ms": {k: round(rep[k], 1) for k in ("ms_hamiltonian", "ms_gram", "ms_eigensolve",
+                                                                 "ms_rotate", "ms_vector")}}
+        del X
+    H.close()
+    diff = float(np.abs(evs["fp64"] - evs["bf16x3_gram"]).max())
+    return {"workload": "diamond216_120cube_480of528states_fd8_kinetic_precond", **runs,
+            "max_abs_ev_diff_mixed_vs_fp64_Ha": diff,
+            "speedup_mixed_vs_fp64": round(runs["fp64"]["seconds"] / runs["bf16x3_gram"]["seconds"], 3)}
+
+
 # --------------------------------------------------------------- GPU arm
 def run_gpu_arm(a):
     import numpy as np
@@ -402,8 +444,13 @@ def run_gpu_arm(a):
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
     lob = None
+    lob216 = None
     if rank == 0 and not a.no_lobpcg:
         lob = lobpcg_diamond8(ctx, cpu=(ws == 1 and not a.no_cpu_baseline))
+        if not a.no_lobpcg216:
+            del X, HX
+            torch.cuda.empty_cache()
+            lob216 = lobpcg_diamond216(ctx)
 
     if rank == 0:
         line = {
@@ -433,6 +480,8 @@ def run_gpu_arm(a):
             line["sweep"] = sweep
         if lob:
             line["lobpcg"] = lob
+        if lob216:
+            line["lobpcg_216"] = lob216
         print(json.dumps(line), flush=True)
     H.close()
     ctx.close()

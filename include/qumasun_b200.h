@@ -38,9 +38,10 @@ typedef enum qg_status {
 } qg_status;
 
 /* QG_MIXED_BF16X3 (LOBPCG only): the Gram products run as split-BF16x3 tensor-core
- * GEMMs with FP32 accumulation (FP64 across K chunks); H, residuals, rotations,
- * norms and the small eigensolves stay FP64, and a final FP64 Rayleigh-Ritz on X
- * sets the returned eigenpairs. */
+ * GEMMs with FP32 accumulation (FP64 across 1024-row K chunks) until the residual
+ * falls below 1e-6 or stops halving, then as FP64; H, residuals, rotations, norms
+ * and the small eigensolves stay FP64 throughout (a solve that ends while still
+ * mixed takes a final FP64 Rayleigh-Ritz on X). */
 typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2 } qg_precision;
 
 typedef struct qg_context_s* qg_context;
@@ -197,6 +198,8 @@ typedef struct qg_lobpcg_report {
     int restarts;       /* iterations whose [x r p] Gram matrix was not positive definite at
                            working precision and that were solved on its numerically
                            nonsingular subspace (eigenvalues of B above 1e-12 max) */
+    int mixed_iterations; /* QG_MIXED_BF16X3: iterations run with BF16x3 Gram products before
+                           the hand-over to FP64 (residual below 1e-6 or stalled 3 iterations) */
 } qg_lobpcg_report;
 
 /* Block LOBPCG for the ns lowest eigenpairs of H, FP64 on the GPU.
@@ -236,6 +239,14 @@ int qg_lobpcg_z(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double
 /* Same with DEVICE buffers X and P (ld = 2N); ev stays a host array. */
 int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
                        double* X, double* P, qg_lobpcg_report* report);
+
+/* No counterpart in the reference (its Gram products are FP64 BLAS, w_dgemm.h:32-36).
+ * C (m x m, column-major, ld m) = alpha * A^T B for DEVICE blocks A, B (N x m,
+ * ld N; B NULL means B = A) through the mixed-precision path of
+ * QG_MIXED_BF16X3: split-BF16x3 tensor-core products with FP32 accumulation
+ * over K chunks and FP64 accumulation across chunks. Waits for the stream. */
+int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
+                    double* C);
 
 /* Batched small generalised eigensolver, FP64, DEVICE pointers, context stream:
  * for b < batch, A_b z = lambda B_b z with A_b = A + b*stride, B_b = B + b*stride

@@ -26,14 +26,14 @@ __global__ void k_split_bf16(const double* __restrict__ src, long long n, __nv_b
     }
 }
 
-// C[e] = alpha * sum_c P[c][e] for e < m*m, chunks in order.
-__global__ void k_reduce_chunks(const float* __restrict__ P, int nchunk, long long mm, double alpha,
+// C[e] (+)= alpha * sum_c P[c][e] for e < m*m, chunks in order (accumulate: add to C).
+__global__ void k_reduce_chunks(const float* __restrict__ P, int nchunk, long long mm, double alpha, int accumulate,
                                 double* __restrict__ C) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < mm; e += stride) {
         double s = 0.0;
         for (int c = 0; c < nchunk; ++c) s += (double)P[(long long)c * mm + e];
-        C[e] = alpha * s;
+        C[e] = accumulate ? C[e] + alpha * s : alpha * s;
     }
 }
 
@@ -56,8 +56,8 @@ int MixedGram::setup(long long N_, int mmax_) {
     QG_TRY(split_b.reserve(2 * elems * sizeof(__nv_bfloat16)));
     nfull = (int)(N / kChunk);
     rem = (int)(N - (long long)nfull * kChunk);
-    const int nparts = nfull + (rem ? 1 : 0);
-    QG_TRY(part.reserve((size_t)nparts * mmax * mmax * sizeof(float)));
+    const int nparts = std::min(nfull, kBatch) + (rem ? 1 : 0);
+    QG_TRY(part.reserve((size_t)std::max(nparts, 1) * mmax * mmax * sizeof(float)));
     return QG_OK;
 }
 
@@ -82,22 +82,33 @@ int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, do
     const __nv_bfloat16* As[3] = {ahi, ahi, alo};
     const __nv_bfloat16* Bs[3] = {bhi, blo, bhi};
     QG_MG_BLAS_TRY(cublasSetStream(blas, st));
-    for (int t = 0; t < 3; ++t) {
-        const float* beta = t == 0 ? &zero : &one;
-        if (nfull > 0)
-            QG_MG_BLAS_TRY(cublasGemmStridedBatchedEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, kChunk, &one, As[t],
-                                                      CUDA_R_16BF, (int)N, kChunk, Bs[t], CUDA_R_16BF, (int)N, kChunk,
-                                                      beta, P, CUDA_R_32F, m, mm, nfull, CUBLAS_COMPUTE_32F,
-                                                      CUBLAS_GEMM_DEFAULT));
-        if (rem)
-            QG_MG_BLAS_TRY(cublasGemmEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, rem, &one,
-                                        As[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N,
-                                        Bs[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N, beta,
-                                        P + (long long)nfull * mm, CUDA_R_32F, m, CUBLAS_COMPUTE_32F,
-                                        CUBLAS_GEMM_DEFAULT));
-    }
     if (ldc != m) return QG_ERR_INVALID;
-    k_reduce_chunks<<<148 * 4, 256, 0, st>>>(P, nfull + (rem ? 1 : 0), mm, alpha, C);
+    // batches of up to kBatch chunks: three FP32-accumulated products per chunk, then
+    // the batch's chunk partials are added into C in FP64
+    bool first = true;
+    for (int c0 = 0; c0 < nfull || (first && rem); c0 += kBatch) {
+        const int nb = std::max(0, std::min(kBatch, nfull - c0));
+        const bool last = c0 + kBatch >= nfull;
+        const int tail = (last && rem) ? 1 : 0;
+        for (int t = 0; t < 3; ++t) {
+            const float* beta = t == 0 ? &zero : &one;
+            const long long k0 = (long long)c0 * kChunk;
+            if (nb > 0)
+                QG_MG_BLAS_TRY(cublasGemmStridedBatchedEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, kChunk, &one,
+                                                          As[t] + k0, CUDA_R_16BF, (int)N, kChunk, Bs[t] + k0,
+                                                          CUDA_R_16BF, (int)N, kChunk, beta, P, CUDA_R_32F, m, mm, nb,
+                                                          CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+            if (tail)
+                QG_MG_BLAS_TRY(cublasGemmEx(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, rem, &one,
+                                            As[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N,
+                                            Bs[t] + (long long)nfull * kChunk, CUDA_R_16BF, (int)N, beta,
+                                            P + (long long)nb * mm, CUDA_R_32F, m, CUBLAS_COMPUTE_32F,
+                                            CUBLAS_GEMM_DEFAULT));
+        }
+        k_reduce_chunks<<<148 * 4, 256, 0, st>>>(P, nb + tail, mm, alpha, first ? 0 : 1, C);
+        first = false;
+        if (last) break;
+    }
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
 }
@@ -109,3 +120,30 @@ void MixedGram::release() {
 }
 
 }  // namespace qg
+
+namespace {
+struct CtxGram {
+    qg::MixedGram mg;
+};
+}  // namespace
+
+int qg_blas_handle(qg_context c, cublasHandle_t* out);
+
+extern "C" {
+
+int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha, double* C) {
+    if (!ctx || N <= 0 || m <= 0 || !A || !C) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(ctx->device));
+    cublasHandle_t blas;
+    QG_TRY(qg_blas_handle(ctx, &blas));
+    CtxGram g;
+    QG_TRY(g.mg.setup(N, m));
+    QG_TRY(g.mg.split(A, m, 0, ctx->stream));
+    const bool same = (B == nullptr || B == A);
+    if (!same) QG_TRY(g.mg.split(B, m, 1, ctx->stream));
+    QG_TRY(g.mg.gram(blas, ctx->stream, m, same, alpha, C, m));
+    QG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return QG_OK;
+}
+
+}  // extern "C"

@@ -7,7 +7,12 @@
 namespace qg {
 
 struct MixedGram {
-    static constexpr int kChunk = 13824;  // K rows per FP32-accumulated chunk
+    // K rows per FP32-accumulated chunk. The tensor cores' FP32 accumulation of
+    // same-sign terms drifts by about kChunk * 4e-9 of the sum (a Gram diagonal over
+    // 1.7M rows lost 5e-5 with 13824-row chunks), so chunks stay short and their
+    // partials are summed in FP64, kBatch chunks per batched GEMM call.
+    static constexpr int kChunk = 1024;
+    static constexpr int kBatch = 96;
     long long N = 0;
     int mmax = 0, nfull = 0, rem = 0;
     DevBuf split_a, split_b, part;

@@ -592,6 +592,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     int restarts = 0;
     const int c = comps;
     const int nconv = (opt->n_converge > 0 && opt->n_converge < n) ? opt->n_converge : n;
+    double best_res = 1e300;
+    int best_it = 0, mixed_iters = s.mixed ? opt->max_iter : 0;
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
@@ -658,11 +660,25 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             ++it;
             break;
         }
-        if (opt->verbose) printf("lobpcg iter %d max residual %.3e\n", it + 1, maxres);
-        if (maxres < tol * s.dV) {
+        if (opt->verbose) printf("lobpcg iter %d max residual %.3e%s\n", it + 1, maxres, s.mixed ? " (bf16x3)" : "");
+        if (maxres < tol * s.dV && !s.mixed) {
             converged = true;
             ++it;
             break;
+        }
+        // mixed precision: the BF16x3 Gram products carry ~5e-6 relative errors, which
+        // stall the residual near 1e-6; hand over to FP64 Gram products once the residual
+        // is below that level or has not halved over three iterations
+        if (s.mixed) {
+            if (maxres < best_res * 0.5) {
+                best_res = maxres;
+                best_it = it;
+            }
+            if (maxres < 1e-6 || it - best_it >= 3) {
+                s.mixed = false;
+                s.trunc_eps = 1e-12;
+                mixed_iters = it + 1;
+            }
         }
     }
     // mixed precision: a final FP64 Rayleigh-Ritz on X alone (FP64 Gram of [x], sygvd,
@@ -713,6 +729,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         rep->ms_rotate = tm.acc[3];
         rep->ms_vector = tm.acc[4];
         rep->restarts = restarts;
+        rep->mixed_iterations = std::min(mixed_iters, it);
     }
     const int dstat = qg_context_take_device_status(h->ctx);
     if (dstat != QG_OK) return dstat;

@@ -74,7 +74,7 @@ class LobpcgReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("max_residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_hamiltonian", C.c_double), ("ms_gram", C.c_double),
                 ("ms_eigensolve", C.c_double), ("ms_rotate", C.c_double), ("ms_vector", C.c_double),
-                ("restarts", C.c_int)]
+                ("restarts", C.c_int), ("mixed_iterations", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -118,6 +118,7 @@ def lib():
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
+        L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp]
         L.qg_lobpcg_z.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_lobpcg_z_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]

@@ -69,3 +69,17 @@ def test_gamma_point_complex_solver_matches_real_solver(cuda_ctx):
     r = solve(cuda_ctx, cell, (0.0, 0.0, 0.0), X0, max_iter=3000)
     assert r["status"] == 0
     np.testing.assert_allclose(np.sort(r["ev"]), np.sort(g["ev"]), rtol=0, atol=TOL_EV)
+
+
+def test_diamond8_kpoint_mixed_precision(cuda_ctx, gold):
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell()
+    g = tuple(gold["d8_g"])
+    X0 = initial_states(int(gold["d8_ns"]), 2 * cell.N, seed=int(gold["d8_seed"]))
+    H = Hamiltonian(cuda_ctx, cell, kvec=g)
+    X = torch.from_numpy(X0).cuda()
+    r = H.lobpcg_device(X, None, max_iter=400, precond=1, precision=2, tol=1e-12, complex_states=True)
+    H.close()
+    assert r["status"] == 0 and r["report"]["converged"] == 1
+    np.testing.assert_allclose(np.sort(r["ev"]), gold["d8_lanczos"][:16], rtol=0, atol=TOL_EV)
