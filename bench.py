@@ -19,6 +19,7 @@ divided by the max over ranks of the device time.
 from __future__ import annotations
 
 import argparse
+import math
 import json
 import os
 import subprocess
@@ -52,6 +53,10 @@ def parse():
                    help="skip the 216-atom 120^3 LOBPCG leg (FP64 vs BF16x3 Gram, about a minute)")
     p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
+    p.add_argument("--no-kpoint", action="store_true", help="skip the k-point leg (64 Monkhorst-Pack points)")
+    p.add_argument("--only", choices=["kpoint"], default=None,
+                   help="run one leg alone and print its JSON (profiling captures)")
+    p.add_argument("--kpoints", type=int, default=64, help="k-points of the k-point leg (4x4x4 grid order)")
     return p.parse_args()
 
 
@@ -275,6 +280,73 @@ def lobpcg_diamond8(ctx, cpu=True):
     return out
 
 
+def monkhorst_pack(n, a0):
+    """n x n x n Monkhorst-Pack Bloch vectors (bohr^-1) of a cubic cell with edge a0:
+    k = (2r - n - 1) / (2n) * 2 pi / a0 per axis, r = 1..n."""
+    f = [(2 * r - n - 1) / (2 * n) for r in range(1, n + 1)]
+    b = 2 * math.pi / a0
+    return [(b * fx, b * fy, b * fz) for fz in f for fy in f for fx in f]
+
+
+def kpoint_leg(ctx, n_k=64, steps=10):
+    """Complex k-point operator on the 8-atom 40^3 cell, 16 states per k-point, over a
+    4x4x4 Monkhorst-Pack grid: (1) H_k|psi> throughput of the complex apply, (2) time to
+    the 16 lowest eigenpairs at every k-point (FP64 complex LOBPCG, kinetic
+    preconditioner, k-points one after another through qg_hamiltonian_set_kvector)."""
+    import numpy as np
+    import torch
+    from qumasun_b200 import Hamiltonian
+    from qumasun_b200.cell import build_cell
+    cell = build_cell()
+    N, ns = cell.N, 16
+    mp = monkhorst_pack(4, 6.74)
+    ks = mp[:n_k]
+    H = Hamiltonian(ctx, cell, kvec=mp[0])
+    gen = torch.Generator(device="cuda").manual_seed(77)
+    X = torch.rand(ns, 2 * N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    HX = torch.empty_like(X)
+    for _ in range(3):
+        H.apply_z(X, HX)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        H.apply_z(X, HX)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    phases = sorted((H.apply_timed_z(ns, X.data_ptr(), HX.data_ptr()) for _ in range(5)), key=lambda p: p[1])[2]
+    nbytes = N * ns * 32 + N * 8
+    apply = {"ms": round(ms, 4), "GBs": round(nbytes / (ms * 1e-3) / 1e9, 1),
+             "state_apps_per_s": round(ns / (ms * 1e-3), 1),
+             "phase_ms": {"projection": round(phases[0], 4), "stencil_V": round(phases[1], 4),
+                          "scatter": round(phases[2], 4)}}
+    solves = None
+    if n_k > 0:
+        from qumasun_b200.cell import initial_states
+        X0 = initial_states(ns, 2 * N, seed=1234)
+        evs, its = [], []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        for k in ks:
+            H.set_kvector(k)
+            r = H.lobpcg_z(X0, max_iter=500, precond=1, tol=1e-10)
+            evs.append(r["ev"])
+            its.append(r["report"]["iterations"])
+            dev_ms += r["report"]["ms_total"]
+        wall = time.perf_counter() - t0
+        evs = np.array(evs)
+        # time reversal: E(k) = E(-k); the Monkhorst-Pack grid holds both of each pair
+        pair = float(max(np.abs(np.sort(evs[i]) - np.sort(evs[n_k - 1 - i])).max() for i in range(n_k)))
+        solves = {"k_points": n_k, "states_per_k": ns, "seconds": round(wall, 3), "device_ms": round(dev_ms, 1),
+                  "iterations_max": int(max(its)), "iterations_mean": round(float(np.mean(its)), 1),
+                  "band_min_Ha": float(evs.min()), "band_max_Ha": float(evs.max()),
+                  "max_abs_ev_diff_k_vs_minus_k_Ha": pair}
+    H.close()
+    return {"workload": "diamond8_40cube_16states_mp4x4x4_fd8_complex", "apply": apply, "lobpcg": solves}
+
+
 def lobpcg_diamond216(ctx):
     """Time to the 480 lowest eigenpairs (528 solved, a 48-state guard band) of the
     216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
@@ -443,6 +515,9 @@ def run_gpu_arm(a):
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
+    kp = None
+    if rank == 0 and not a.no_kpoint:
+        kp = kpoint_leg(ctx, n_k=a.kpoints)
     lob = None
     lob216 = None
     if rank == 0 and not a.no_lobpcg:
@@ -482,6 +557,8 @@ def run_gpu_arm(a):
             line["lobpcg"] = lob
         if lob216:
             line["lobpcg_216"] = lob216
+        if kp:
+            line["kpoint"] = kp
         print(json.dumps(line), flush=True)
     H.close()
     ctx.close()
@@ -491,10 +568,24 @@ def run_gpu_arm(a):
     return 0
 
 
+def run_only(a):
+    import torch
+    from qumasun_b200 import Context
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    ctx.use_torch_stream()
+    out = kpoint_leg(ctx, n_k=a.kpoints, steps=a.steps)
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference_arm(a)
+    if a.only:
+        return run_only(a)
     return run_gpu_arm(a)
 
 
