@@ -242,11 +242,13 @@ int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns,
 
 /* No counterpart in the reference (its Gram products are FP64 BLAS, w_dgemm.h:32-36).
  * C (m x m, column-major, ld m) = alpha * A^T B for DEVICE blocks A, B (N x m,
- * ld N; B NULL means B = A) through the mixed-precision path of
- * QG_MIXED_BF16X3: split-BF16x3 tensor-core products with FP32 accumulation
- * over K chunks and FP64 accumulation across chunks. Waits for the stream. */
+ * ld N; B NULL means B = A) through the mixed-precision Gram of QG_MIXED_BF16X3:
+ * pieces = 2 or 3 bf16 pieces per value on the library's tcgen05 kernel (FP32
+ * accumulation over one 64-row K block, FP64 across blocks; N a multiple of 8),
+ * pieces = 0 the cuBLAS BF16 hi/lo path (FP32 over 1024-row chunks). Waits for
+ * the stream; returns QG_ERR_UNSUPPORTED if the tcgen05 path cannot take N. */
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
-                    double* C);
+                    double* C, int pieces);
 
 /* Batched small generalised eigensolver, FP64, DEVICE pointers, context stream:
  * for b < batch, A_b z = lambda B_b z with A_b = A + b*stride, B_b = B + b*stride

@@ -48,9 +48,12 @@ __global__ void k_reduce_chunks(const float* __restrict__ P, int nchunk, long lo
 
 }  // namespace
 
-int MixedGram::setup(long long N_, int mmax_) {
+int MixedGram::setup(long long N_, int mmax_, int pieces_) {
     N = N_;
     mmax = mmax_;
+    pieces = pieces_;
+    use_tc = pieces > 0 && TcGram::supported(N);
+    if (use_tc) return tc.setup(N, mmax, pieces);
     const size_t elems = (size_t)N * mmax;
     QG_TRY(split_a.reserve(2 * elems * sizeof(__nv_bfloat16)));
     QG_TRY(split_b.reserve(2 * elems * sizeof(__nv_bfloat16)));
@@ -62,6 +65,7 @@ int MixedGram::setup(long long N_, int mmax_) {
 }
 
 int MixedGram::split(const double* A, int m, int which, cudaStream_t st) {
+    if (use_tc) return tc.split(A, m, which, st);
     const long long n = N * m;
     DevBuf& b = which == 0 ? split_a : split_b;
     __nv_bfloat16* hi = b.as<__nv_bfloat16>();
@@ -71,7 +75,9 @@ int MixedGram::split(const double* A, int m, int which, cudaStream_t st) {
     return QG_OK;
 }
 
-int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, double alpha, double* C, int ldc) {
+int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, double* C,
+                    int ldc, int* err) {
+    if (use_tc) return tc.gram(st, m, b_is_a, lower, alpha, C, ldc, err);
     const __nv_bfloat16* ahi = split_a.as<__nv_bfloat16>();
     const __nv_bfloat16* alo = ahi + (size_t)N * mmax;
     const __nv_bfloat16* bhi = b_is_a ? ahi : split_b.as<__nv_bfloat16>();
@@ -114,6 +120,7 @@ int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, do
 }
 
 void MixedGram::release() {
+    tc.release();
     split_a.release();
     split_b.release();
     part.release();
@@ -131,19 +138,20 @@ int qg_blas_handle(qg_context c, cublasHandle_t* out);
 
 extern "C" {
 
-int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha, double* C) {
-    if (!ctx || N <= 0 || m <= 0 || !A || !C) return QG_ERR_INVALID;
+int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha, double* C,
+                    int pieces) {
+    if (!ctx || N <= 0 || m <= 0 || !A || !C || pieces < 0 || pieces > 3 || pieces == 1) return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(ctx->device));
     cublasHandle_t blas;
     QG_TRY(qg_blas_handle(ctx, &blas));
     CtxGram g;
-    QG_TRY(g.mg.setup(N, m));
+    QG_TRY(g.mg.setup(N, m, pieces));
     QG_TRY(g.mg.split(A, m, 0, ctx->stream));
     const bool same = (B == nullptr || B == A);
     if (!same) QG_TRY(g.mg.split(B, m, 1, ctx->stream));
-    QG_TRY(g.mg.gram(blas, ctx->stream, m, same, alpha, C, m));
+    QG_TRY(g.mg.gram(blas, ctx->stream, m, same, false, alpha, C, m, ctx->dev_status));
     QG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return QG_OK;
+    return qg_context_take_device_status(ctx);
 }
 
 }  // extern "C"

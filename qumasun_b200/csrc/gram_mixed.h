@@ -2,6 +2,7 @@
 #pragma once
 #include <cublas_v2.h>
 
+#include "gram_tc.h"
 #include "qg_internal.h"
 
 namespace qg {
@@ -16,12 +17,19 @@ struct MixedGram {
     long long N = 0;
     int mmax = 0, nfull = 0, rem = 0;
     DevBuf split_a, split_b, part;
+    // pieces > 0: the tcgen05 kernel with that many bf16 pieces (gram_tc.cu);
+    // 0 (or a row count that is not a multiple of 8): cuBLAS BF16 GEMMs on hi/lo pieces
+    int pieces = 3;
+    bool use_tc = false;
+    TcGram tc;
 
-    int setup(long long N, int mmax);
-    // bf16 hi/lo copies of the N x m block A (ld N) into slot `which` (0: A side, 1: B side)
+    int setup(long long N, int mmax, int pieces = 3);
+    // bf16 pieces of the N x m block A (ld N) into slot `which` (0: A side, 1: B side)
     int split(const double* A, int m, int which, cudaStream_t st);
-    // C (m x m, ld m) = alpha * A^T B from the split slots (B = A when b_is_a)
-    int gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, double alpha, double* C, int ldc);
+    // C (m x m, ld m) = alpha * A^T B from the split slots (B = A when b_is_a); lower:
+    // only the lower triangle is needed (the tcgen05 kernel then skips the upper tiles)
+    int gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, double* C,
+             int ldc, int* err);
     void release();
     ~MixedGram() { release(); }
 };

@@ -387,8 +387,8 @@ struct Solver {
         if (mixed) {
             QG_TRY(mg.split(x, m, 0, st));
             QG_TRY(mg.split(Ax, m, 1, st));
-            QG_TRY(mg.gram(blas, st, m, false, dV, Sa, m));
-            QG_TRY(mg.gram(blas, st, m, true, dV, Sb, m));
+            QG_TRY(mg.gram(blas, st, m, false, c == 1, dV, Sa, m, h->ctx->dev_status));
+            QG_TRY(mg.gram(blas, st, m, true, c == 1, dV, Sb, m, h->ctx->dev_status));
             return QG_OK;
         }
         if (c == 2) {
@@ -504,6 +504,32 @@ struct Solver {
             *Zout = M;
             *ldz = 2 * k3;
         }
+        QG_CUDA_TRY(cudaGetLastError());
+        return QG_OK;
+    }
+
+    // FP64 Rayleigh-Ritz on X alone: the n x n pencil (X^T AX dV, X^T X dV) from FP64
+    // products, x <- x Z, Ax = H x, Rayleigh quotients and residuals. Leaves the
+    // residual norms in nr_d.
+    int rayleigh_ritz_x() {
+        const bool was_mixed = mixed;
+        const double te = trunc_eps;
+        mixed = false;
+        trunc_eps = 1e-12;
+        QG_TRY(gram(c * n));
+        const double* Z = nullptr;
+        int ldz = 0, info = 0;
+        QG_TRY(solve_pencil(n, n, n, &Z, &ldz, &info));
+        if (info > 0) QG_TRY(solve_truncated(n, n, &Z, &ldz));
+        else if (info < 0) return QG_ERR_LIBRARY;
+        QG_TRY(gemm_nn(c * n, c * n, x, Z, ldz, Tx, 0.0));
+        QG_CUDA_TRY(cudaMemcpyAsync(x, Tx, (size_t)L * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        normalize(x, nullptr);
+        QG_TRY(applyH(x, Ax));
+        coldot(x, Ax, dV, ev_d);
+        residual();
+        mixed = was_mixed;
+        trunc_eps = te;
         QG_CUDA_TRY(cudaGetLastError());
         return QG_OK;
     }
@@ -661,14 +687,33 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             break;
         }
         if (opt->verbose) printf("lobpcg iter %d max residual %.3e%s\n", it + 1, maxres, s.mixed ? " (bf16x3)" : "");
+        if (s.mixed && maxres < tol * s.dV) {
+            // the mixed iteration reached the tolerance: FP64 Rayleigh-Ritz on X and an
+            // FP64 residual decide; the iteration continues with FP64 Gram products if needed
+            QG_TRY(s.rayleigh_ritz_x());
+            QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (pc) {
+                QG_TRY(pc->apply(s.r, st));
+                s.normalize(s.r, nullptr);
+            }
+            QG_CUDA_TRY(cudaStreamSynchronize(st));
+            maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
+            s.mixed = false;
+            s.trunc_eps = 1e-12;
+            mixed_iters = it + 1;
+            if (opt->verbose) printf("lobpcg FP64 Rayleigh-Ritz on X: max residual %.3e\n", maxres);
+        }
         if (maxres < tol * s.dV && !s.mixed) {
             converged = true;
             ++it;
             break;
         }
-        // mixed precision: the BF16x3 Gram products carry ~5e-6 relative errors, which
-        // stall the residual near 1e-6; hand over to FP64 Gram products once the residual
-        // is below that level or has not halved over three iterations
+        // mixed precision: hand over to FP64 Gram products once the residual is below
+        // 1e-6 or has not halved over three iterations. The split-BF16 pencil is solved
+        // on the span of B's eigenvectors above 1e-6 max (its error level); from about
+        // that residual on, FP64 products converge the tail in fewer iterations than
+        // mixed ones with either a looser or a tighter floor (216-atom cell: 19 + 13
+        // iterations against 42 + 22 when the hand-over waits for a stall near 1e-9)
         if (s.mixed) {
             if (maxres < best_res * 0.5) {
                 best_res = maxres;
@@ -681,29 +726,14 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             }
         }
     }
-    // mixed precision: a final FP64 Rayleigh-Ritz on X alone (FP64 Gram of [x], sygvd,
-    // FP64 rotation, Ax re-applied, residual) fixes the eigenvalues to FP64 accuracy
+    // a solve that ends while still mixed takes a final FP64 Rayleigh-Ritz on X
     if (s.mixed && status == QG_OK) {
         s.mixed = false;
-        s.trunc_eps = 1e-12;
-        QG_TRY(s.gram(c * n));
-        const double* Z = nullptr;
-        int ldz = 0, info = 0;
-        QG_TRY(s.solve_pencil(n, n, n, &Z, &ldz, &info));
-        if (info > 0) QG_TRY(s.solve_truncated(n, n, &Z, &ldz));
-        else if (info < 0) status = QG_ERR_LIBRARY;
-        if (status == QG_OK) {
-            QG_TRY(s.gemm_nn(c * n, c * n, s.x, Z, ldz, s.Tx, 0.0));
-            QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
-            s.normalize(s.x, nullptr);
-            QG_TRY(s.applyH(s.x, s.Ax));
-            s.coldot(s.x, s.Ax, s.dV, s.ev_d);
-            s.residual();
-            QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-            QG_CUDA_TRY(cudaStreamSynchronize(st));
-            maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
-            converged = maxres < tol * s.dV;
-        }
+        QG_TRY(s.rayleigh_ritz_x());
+        QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
+        converged = maxres < tol * s.dV;
     }
     // outputs
     QG_CUDA_TRY(cudaMemcpyAsync(ev_h.data(), s.ev_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -118,7 +118,7 @@ def lib():
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
-        L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp]
+        L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp, C.c_int]
         L.qg_lobpcg_z.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_lobpcg_z_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
