@@ -1,15 +1,18 @@
 """Split-BF16 Gram products (qg_gram_mixed_d) against FP64 DGEMM on the device.
 pieces = 3 and 2 run the library's tcgen05 kernel (FP32 accumulation over one
 64-row K block, FP64 across blocks); pieces = 0 the cuBLAS BF16 hi/lo path with
-1024-row FP32 chunks. Bounds (max abs error on unit-norm columns): 3 pieces 5e-8,
-2 pieces (a_lo b_lo dropped, ~2^-18 on diagonal-like entries) 1e-5, cuBLAS 1e-5."""
+1024-row FP32 chunks. Bounds (max abs error on unit-norm columns): products of
+unrelated columns (A^T B) 5e-8 with 3 pieces; norm-like entries (A^T A, same-sign
+sums) carry the tensor cores' FP32 accumulation drift, ~7 ulp of the K block's
+partial sum, so 2e-6 with 3 pieces; 2 pieces (a_lo b_lo dropped, ~2^-18 on
+norm-like entries) and the cuBLAS path 1e-5."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-BOUND = {3: 5e-8, 2: 1e-5, 0: 1e-5}
+BOUND = {3: (5e-8, 2e-6), 2: (1e-5, 1e-5), 0: (1e-5, 1e-5)}
 
 
 def run_gram(ctx, A, B, pieces):
@@ -33,12 +36,12 @@ def test_gram_mixed_matches_fp64(cuda_ctx, N, m, pieces):
     B = torch.rand(m, N, dtype=torch.float64, device="cuda", generator=g) - 0.5
     A /= A.norm(dim=1, keepdim=True)
     B /= B.norm(dim=1, keepdim=True)
-    for Bt in (B, A):
+    for case, Bt in enumerate((B, A)):
         C64 = run_gram(cuda_ctx, A, Bt, pieces)
         ref = (A @ Bt.T).T  # column-major C(i, j) = a_i . b_j is C64[j, i] in row-major torch
         err = (C64 - ref).abs().max().item()
         print(N, m, pieces, "max abs error", err)
-        assert err < BOUND[pieces]
+        assert err < BOUND[pieces][case]
 
 
 def test_gram_cublas_path_takes_any_row_count(cuda_ctx):
