@@ -46,6 +46,7 @@ typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2 } qg_p
 
 typedef struct qg_context_s* qg_context;
 typedef struct qg_hamiltonian_s* qg_hamiltonian;
+typedef struct qg_learned_s* qg_learned;
 
 /*
  * Hamiltonian description. The projector tables are the reference's own
@@ -249,6 +250,39 @@ int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns,
  * the stream; returns QG_ERR_UNSUPPORTED if the tcgen05 path cannot take N. */
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
                     double* C, int pieces);
+
+/* ---- learned preconditioner ------------------------------------------------
+ * No counterpart in the reference (its solvers are unpreconditioned). A 4-layer
+ * periodic 3D convolutional network (3^3 kernels, channels 2 -> 16 -> 16 -> 16 -> 1,
+ * ReLU after the first three, BF16 weights and activations, FP32 accumulation):
+ *   NN(r) = rms(r) * net([r / rms(r), V / vscale]),  rms(r) = sqrt(mean r^2),
+ * used by LOBPCG (precond = 2) as w = T r + NN(r), T the kinetic preconditioner.
+ * Parameters: qg_learned_num_params() floats, per layer the weights [cout][cin][27]
+ * (taps x fastest) followed by the cout biases. A new network has all parameters
+ * zero (NN = 0). The handle counts as an operator of its context. */
+int qg_learned_num_params(void);
+int qg_learned_create(qg_context ctx, qg_learned* out);
+int qg_learned_destroy(qg_learned nn);
+int qg_learned_set_params(qg_learned nn, const float* params, int n);  /* HOST params */
+int qg_learned_get_params(qg_learned nn, float* params, int n);
+/* out[s] (+)= NN(R[s]) for ns states on an nx x ny x nz grid; R, V, out DEVICE FP64. */
+int qg_learned_apply_d(qg_learned nn, int nx, int ny, int nz, int ns, const double* R, long long ldr,
+                       const double* V, double vscale, double* out, long long ldo, int accumulate);
+/* Loss sum_s |net_s - Y[s]/rms(R[s])|^2 / sum_s |Y[s]/rms(R[s])|^2 of a batch (Y: the wanted
+ * NN(R) in the units of R, DEVICE FP64) and its gradient (grad_host: HOST, num_params
+ * floats, may be NULL); waits for the stream. */
+int qg_learned_gradient(qg_learned nn, int nx, int ny, int nz, int ns, const double* R, long long ldr,
+                        const double* V, double vscale, const double* Y, long long ldy, double* loss,
+                        float* grad_host);
+/* qg_learned_gradient followed by one Adam step (beta 0.9 / 0.999) with learning rate lr. */
+int qg_learned_train_step(qg_learned nn, int nx, int ny, int nz, int ns, const double* R, long long ldr,
+                          const double* V, double vscale, const double* Y, long long ldy, float lr,
+                          double* loss);
+/* R[s] <- T R[s] in place, T = (-1/2 Lap_FD + shift)^-1 the kinetic preconditioner of
+ * LOBPCG's precond = 1 (DEVICE R, ns states, ldr = N). */
+int qg_hamiltonian_precondition_d(qg_hamiltonian ham, int ns, double* R, long long ldr, double shift);
+/* Attaches a network to an operator for LOBPCG's precond = 2 (NULL detaches). */
+int qg_hamiltonian_set_learned(qg_hamiltonian ham, qg_learned nn, double vscale);
 
 /* Batched small generalised eigensolver, FP64, DEVICE pointers, context stream:
  * for b < batch, A_b z = lambda B_b z with A_b = A + b*stride, B_b = B + b*stride

@@ -550,7 +550,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
     if (comps == 2 && h->order != 8) return QG_ERR_UNSUPPORTED;
     if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3) return QG_ERR_UNSUPPORTED;
-    if (opt->precond != 0 && opt->precond != 1) return QG_ERR_INVALID;
+    if (opt->precond < 0 || opt->precond > 2) return QG_ERR_INVALID;
+    if (opt->precond == 2 && !h->learned) return QG_ERR_INVALID;
     const long long N = h->N();
     if ((long long)n * 3 > N) return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
@@ -596,14 +597,24 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     s.coldot(s.x, s.Ax, s.dV, s.ev_d);
     s.residual();
     qg::KineticPrecond* pc = nullptr;
-    if (opt->precond == 1) {
+    const bool learned = opt->precond == 2;
+    // w = T r (precond 1), w = T r + NN(r) (precond 2: the learned correction, learned.cu)
+    auto precondition = [&]() -> int {
+        if (learned) QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.r, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_TRY(pc->apply(s.r, st));
+        if (learned)
+            QG_TRY(qg_learned_apply_d(h->learned, h->nx, h->ny, h->nz, comps * n, s.Tx, N, h->V_d, h->learned_vscale,
+                                      s.r, N, 1));
+        s.normalize(s.r, nullptr);
+        return QG_OK;
+    };
+    if (opt->precond >= 1) {
         // Gamma-point FD symbol on every real column (for k-point states it is an
         // approximation of the k-shifted kinetic operator, still a valid preconditioner)
         if (!h->precond) h->precond = new qg::KineticPrecond();
         pc = h->precond;
         QG_TRY(pc->setup(h, comps * n, opt->precond_shift > 0 ? opt->precond_shift : 1.0));
-        QG_TRY(pc->apply(s.r, st));
-        s.normalize(s.r, nullptr);
+        QG_TRY(precondition());
     } else {
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, 1.0, n, s.f_d);
         s.scale_cols(s.r, nullptr);
@@ -672,10 +683,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         s.residual();
         QG_CUDA_TRY(cudaGetLastError());
         QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-        if (pc) {  // next search direction w = T r, normalised (the residual norms are already taken)
-            QG_TRY(pc->apply(s.r, st));
-            s.normalize(s.r, nullptr);
-        }
+        if (pc) QG_TRY(precondition());  // next search direction, normalised (residual norms already taken)
         tm.mark(5, st);
         tm.mark(-1, st);
         QG_CUDA_TRY(cudaStreamSynchronize(st));
@@ -692,10 +700,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             // FP64 residual decide; the iteration continues with FP64 Gram products if needed
             QG_TRY(s.rayleigh_ritz_x());
             QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-            if (pc) {
-                QG_TRY(pc->apply(s.r, st));
-                s.normalize(s.r, nullptr);
-            }
+            if (pc) QG_TRY(precondition());
             QG_CUDA_TRY(cudaStreamSynchronize(st));
             maxres = *std::max_element(nr_h.begin(), nr_h.begin() + nconv);
             s.mixed = false;

@@ -114,3 +114,11 @@ int KineticPrecond::apply(double* R, cudaStream_t st) {
 }
 
 }  // namespace qg
+
+extern "C" int qg_hamiltonian_precondition_d(qg_hamiltonian h, int ns, double* R, long long ldr, double shift) {
+    if (!h || ns <= 0 || !R || ldr != h->N() || !(shift > 0)) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    if (!h->precond) h->precond = new qg::KineticPrecond();
+    QG_TRY(h->precond->setup(h, ns, shift));
+    return h->precond->apply(R, h->ctx->stream);
+}

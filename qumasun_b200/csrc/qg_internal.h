@@ -105,6 +105,8 @@ struct qg_hamiltonian_s {
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
     qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
+    qg_learned learned = nullptr;           // network of precond = 2 (qg_hamiltonian_set_learned)
+    double learned_vscale = 1.0;
     long long N() const { return (long long)nx * ny * nz; }
 };
 

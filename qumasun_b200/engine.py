@@ -119,6 +119,18 @@ def lib():
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp, C.c_int]
+        L.qg_learned_create.argtypes = [vp, C.POINTER(vp)]
+        L.qg_learned_destroy.argtypes = [vp]
+        L.qg_learned_set_params.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+        L.qg_learned_get_params.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+        L.qg_learned_apply_d.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp, C.c_double,
+                                         vp, C.c_longlong, C.c_int]
+        L.qg_learned_gradient.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp, C.c_double,
+                                          vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_float)]
+        L.qg_learned_train_step.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp,
+                                            C.c_double, vp, C.c_longlong, C.c_float, C.POINTER(C.c_double)]
+        L.qg_hamiltonian_set_learned.argtypes = [vp, vp, C.c_double]
+        L.qg_hamiltonian_precondition_d.argtypes = [vp, C.c_int, vp, C.c_longlong, C.c_double]
         L.qg_lobpcg_z.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_lobpcg_z_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
@@ -191,6 +203,72 @@ def sygv_small_batched(ctx, A, B):
                                         k * k, C.c_void_p(w.data_ptr()), C.c_void_p(Z.data_ptr()),
                                         info.ctypes.data_as(_ip)), "qg_sygv_small_batched_d")
     return w, Z.transpose(1, 2), info
+
+
+class LearnedPreconditioner:
+    """The learned LOBPCG preconditioner network (qg_learned_*): 4 periodic 3^3
+    convolutions 2 -> 16 -> 16 -> 16 -> 1 on [r / rms(r), V / vscale]; LOBPCG with
+    precond=2 uses w = T r + rms(r) * net(...). Parameters start at zero."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        check(lib().qg_learned_create(ctx.h, C.byref(self.h)), "qg_learned_create")
+        self.n_params = lib().qg_learned_num_params()
+        ctx.children.add(self)
+
+    def set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().qg_learned_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size),
+              "qg_learned_set_params")
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        check(lib().qg_learned_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size),
+              "qg_learned_get_params")
+        return p
+
+    def apply(self, grid, R, V, vscale, out=None, accumulate=False):
+        """out (+)= NN(R) for float64 CUDA tensors R (ns, N), V (N,)."""
+        import torch
+        if out is None:
+            out = torch.zeros_like(R)
+        self.ctx.use_torch_stream()
+        check(lib().qg_learned_apply_d(self.h, grid[0], grid[1], grid[2], R.shape[0], C.c_void_p(R.data_ptr()),
+                                       R.shape[1], C.c_void_p(V.data_ptr()), float(vscale), C.c_void_p(out.data_ptr()),
+                                       out.shape[1], 1 if accumulate else 0), "qg_learned_apply_d")
+        return out
+
+    def gradient(self, grid, R, V, vscale, Y):
+        """(loss, gradient) of one batch on the device (FP32 gradient, host)."""
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        self.ctx.use_torch_stream()
+        check(lib().qg_learned_gradient(self.h, grid[0], grid[1], grid[2], R.shape[0], C.c_void_p(R.data_ptr()),
+                                        R.shape[1], C.c_void_p(V.data_ptr()), float(vscale), C.c_void_p(Y.data_ptr()),
+                                        Y.shape[1], C.byref(loss), g.ctypes.data_as(C.POINTER(C.c_float))),
+              "qg_learned_gradient")
+        return loss.value, g
+
+    def train_step(self, grid, R, V, vscale, Y, lr):
+        loss = C.c_double()
+        self.ctx.use_torch_stream()
+        check(lib().qg_learned_train_step(self.h, grid[0], grid[1], grid[2], R.shape[0], C.c_void_p(R.data_ptr()),
+                                          R.shape[1], C.c_void_p(V.data_ptr()), float(vscale),
+                                          C.c_void_p(Y.data_ptr()), Y.shape[1], float(lr), C.byref(loss)),
+              "qg_learned_train_step")
+        return loss.value
+
+    def close(self):
+        if self.h:
+            lib().qg_learned_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Hamiltonian:
@@ -350,6 +428,18 @@ class Hamiltonian:
                                                  C.c_void_p(hx_ptr), 2 * self.N, ph),
               "qg_hamiltonian_apply_timed_z")
         return tuple(ph)
+
+    def precondition(self, R, shift=1.0):
+        """R <- T R in place (kinetic preconditioner) for a float64 CUDA tensor (ns, N)."""
+        self.ctx.use_torch_stream()
+        check(lib().qg_hamiltonian_precondition_d(self.h, R.shape[0], C.c_void_p(R.data_ptr()), R.shape[1],
+                                                  float(shift)), "qg_hamiltonian_precondition_d")
+        return R
+
+    def set_learned(self, nn, vscale=4.0):
+        """Attach a LearnedPreconditioner for LOBPCG precond=2 (None detaches)."""
+        check(lib().qg_hamiltonian_set_learned(self.h, nn.h if nn is not None else None, float(vscale)),
+              "qg_hamiltonian_set_learned")
 
     def set_stencil_kernel(self, plain: bool):
         """False: TMA-staged ring kernel where the shape allows (default); True: register-window kernel."""

@@ -1,0 +1,88 @@
+"""Learned preconditioner kernels on the B200 against the CPU oracle
+(oracle/nn_oracle.py, itself checked by finite differences): forward output and
+parameter gradient of the 4-layer periodic 3D convolutional network, training
+progress, and the LOBPCG hook (precond=2). BF16 activations make the device and
+the oracle differ at the 1e-3 level: forward 5e-3, gradient 2e-2 relative (L2)."""
+import numpy as np
+import pytest
+
+import oracle.nn_oracle as NN
+from qumasun_b200.cell import build_cell, initial_states
+
+pytestmark = pytest.mark.gpu
+
+
+def small_case(seed=5, grid=(16, 12, 8), ns=3):
+    rng = np.random.default_rng(seed)
+    N = grid[0] * grid[1] * grid[2]
+    P = rng.normal(0, 0.15, NN.n_params()).astype(np.float32)
+    R = rng.normal(size=(ns, N))
+    V = -4.0 * np.exp(-rng.uniform(0, 3, size=N))
+    Y = rng.normal(size=(ns, N))
+    return grid, P, R, V, Y
+
+
+def test_forward_matches_oracle(cuda_ctx):
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    grid, P, R, V, Y = small_case()
+    nn = LearnedPreconditioner(cuda_ctx)
+    nn.set_params(P)
+    out = nn.apply(grid, torch.from_numpy(R).cuda(), torch.from_numpy(V).cuda(), 4.0).cpu().numpy()
+    ref = NN.apply(P, grid, R, V, 4.0)
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 5e-3
+    # accumulate mode adds onto the output buffer
+    base = torch.ones((R.shape[0], R.shape[1]), dtype=torch.float64, device="cuda")
+    acc = nn.apply(grid, torch.from_numpy(R).cuda(), torch.from_numpy(V).cuda(), 4.0, out=base, accumulate=True)
+    np.testing.assert_allclose(acc.cpu().numpy(), out + 1.0, rtol=0, atol=1e-12)
+    nn.close()
+
+
+def test_gradient_matches_oracle(cuda_ctx):
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    grid, P, R, V, Y = small_case(seed=6)
+    nn = LearnedPreconditioner(cuda_ctx)
+    nn.set_params(P)
+    loss, g = nn.gradient(grid, torch.from_numpy(R).cuda(), torch.from_numpy(V).cuda(), 4.0,
+                          torch.from_numpy(Y).cuda())
+    rl, rg = NN.loss_and_grad(P, grid, R, V, 4.0, Y)
+    assert abs(loss - rl) / rl < 5e-3
+    off = 0
+    for co, ci in ((16, 2), (16, 16), (16, 16), (1, 16)):
+        n = co * ci * 27 + co
+        a, b = g[off:off + n], rg[off:off + n]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 2e-2, off
+        off += n
+    nn.close()
+
+
+def test_training_reduces_loss_on_a_batch(cuda_ctx):
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    from qumasun_b200.learned import init_params
+    grid, _, R, V, Y = small_case(seed=7)
+    nn = LearnedPreconditioner(cuda_ctx)
+    nn.set_params(init_params(0, nn.n_params))
+    Rt, Vt, Yt = torch.from_numpy(R).cuda(), torch.from_numpy(V).cuda(), torch.from_numpy(0.1 * R + 0.05 * Y).cuda()
+    first = nn.train_step(grid, Rt, Vt, 4.0, Yt, 2e-4)
+    for _ in range(100):
+        last = nn.train_step(grid, Rt, Vt, 4.0, Yt, 2e-4)
+    assert last < 0.8 * first
+    nn.close()
+
+
+def test_lobpcg_with_untrained_network_equals_kinetic(cuda_ctx):
+    """A new network is zero, so precond=2 reproduces precond=1 exactly."""
+    from qumasun_b200 import Hamiltonian, LearnedPreconditioner
+    cell = build_cell(grid=(24, 24, 24))
+    X0 = initial_states(6, cell.N, seed=3)
+    H = Hamiltonian(cuda_ctx, cell)
+    nn = LearnedPreconditioner(cuda_ctx)
+    H.set_learned(nn, 4.0)
+    a = H.lobpcg(X0, max_iter=300, precond=1)
+    b = H.lobpcg(X0, max_iter=300, precond=2)
+    assert a["report"]["iterations"] == b["report"]["iterations"]
+    np.testing.assert_allclose(a["ev"], b["ev"], rtol=0, atol=1e-12)
+    H.close()
+    nn.close()
