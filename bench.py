@@ -54,9 +54,11 @@ def parse():
     p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     p.add_argument("--no-kpoint", action="store_true", help="skip the k-point leg (64 Monkhorst-Pack points)")
-    p.add_argument("--only", choices=["kpoint"], default=None,
+    p.add_argument("--only", choices=["kpoint", "gram"], default=None,
                    help="run one leg alone and print its JSON (profiling captures)")
     p.add_argument("--kpoints", type=int, default=64, help="k-points of the k-point leg (4x4x4 grid order)")
+    p.add_argument("--gram-rows", type=int, default=1_728_000, help="rows N of the --only gram leg")
+    p.add_argument("--gram-cols", type=int, default=1584, help="columns m of the --only gram leg")
     return p.parse_args()
 
 
@@ -568,13 +570,53 @@ def run_gpu_arm(a):
     return 0
 
 
+def gram_leg(ctx, N=1_728_000, m=1584, steps=5):
+    """Split-BF16 Gram products of the mixed-precision LOBPCG at the 216-atom cell's
+    shape (N = 120^3 rows, m = 3 x 528 columns): the tcgen05 kernel with 3 and 2
+    pieces and the cuBLAS BF16 path against FP64 DGEMM, time and max error."""
+    import ctypes as C
+    import torch
+    from qumasun_b200.engine import lib
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.rand(m, N, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    A /= A.norm(dim=1, keepdim=True)
+    Cm = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    ref = A @ A.T
+    out = {"N": N, "m": m}
+    for pieces in (3, 2, 0):
+        rc = lib().qg_gram_mixed_d(ctx.h, N, m, C.c_void_p(A.data_ptr()), None, 1.0, C.c_void_p(Cm.data_ptr()), pieces)
+        if rc != 0:
+            out[f"pieces{pieces}"] = {"status": rc}
+            continue
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            lib().qg_gram_mixed_d(ctx.h, N, m, C.c_void_p(A.data_ptr()), None, 1.0, C.c_void_p(Cm.data_ptr()), pieces)
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / steps
+        out[f"pieces{pieces}"] = {"ms": round(sec * 1e3, 2), "max_abs_err": float((Cm - ref).abs().max().item()),
+                                  "effective_TFLOPs": round(2.0 * N * m * m / sec / 1e12, 1)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        torch.mm(A, A.T)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out["fp64_dgemm"] = {"ms": round(ms, 2), "TFLOPs": round(2.0 * N * m * m / (ms * 1e-3) / 1e12, 1)}
+    return out
+
+
 def run_only(a):
     import torch
     from qumasun_b200 import Context
     torch.cuda.set_device(0)
     ctx = Context(0)
     ctx.use_torch_stream()
-    out = kpoint_leg(ctx, n_k=a.kpoints, steps=a.steps)
+    if a.only == "gram":
+        out = gram_leg(ctx, N=a.gram_rows, m=a.gram_cols, steps=a.steps)
+    else:
+        out = kpoint_leg(ctx, n_k=a.kpoints, steps=a.steps)
     print(json.dumps(out), flush=True)
     ctx.close()
     return 0

@@ -73,6 +73,7 @@ int qg_context_destroy(qg_context c) {
     if (c->live_hamiltonians > 0) return QG_ERR_INVALID;
     cudaSetDevice(c->device);
     qg_release_libraries(c);
+    qg_release_gram_cache(c);
     if (c->own_stream) {
         cudaStreamSynchronize(c->own_stream);
         cudaStreamDestroy(c->own_stream);

@@ -128,11 +128,10 @@ void MixedGram::release() {
 
 }  // namespace qg
 
-namespace {
-struct CtxGram {
-    qg::MixedGram mg;
-};
-}  // namespace
+void qg_release_gram_cache(qg_context c) {
+    delete static_cast<qg::MixedGram*>(c->gram_cache);
+    c->gram_cache = nullptr;
+}
 
 int qg_blas_handle(qg_context c, cublasHandle_t* out);
 
@@ -144,12 +143,19 @@ int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const d
     QG_CUDA_TRY(cudaSetDevice(ctx->device));
     cublasHandle_t blas;
     QG_TRY(qg_blas_handle(ctx, &blas));
-    CtxGram g;
-    QG_TRY(g.mg.setup(N, m, pieces));
-    QG_TRY(g.mg.split(A, m, 0, ctx->stream));
+    // the split buffers are kept on the context and rebuilt when the shape or split changes
+    auto* g = static_cast<qg::MixedGram*>(ctx->gram_cache);
+    if (!g || g->N != N || g->mmax < m || g->pieces != pieces) {
+        qg_release_gram_cache(ctx);
+        g = new qg::MixedGram();
+        ctx->gram_cache = g;
+        QG_TRY(g->setup(N, m, pieces));
+    }
+    if (pieces > 0 && !g->use_tc) return QG_ERR_UNSUPPORTED;
+    QG_TRY(g->split(A, m, 0, ctx->stream));
     const bool same = (B == nullptr || B == A);
-    if (!same) QG_TRY(g.mg.split(B, m, 1, ctx->stream));
-    QG_TRY(g.mg.gram(blas, ctx->stream, m, same, false, alpha, C, m, ctx->dev_status));
+    if (!same) QG_TRY(g->split(B, m, 1, ctx->stream));
+    QG_TRY(g->gram(blas, ctx->stream, m, same, false, alpha, C, m, ctx->dev_status));
     QG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return qg_context_take_device_status(ctx);
 }

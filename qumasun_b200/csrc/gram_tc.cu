@@ -433,14 +433,13 @@ int TcGram::setup(long long N_, int mmax_, int pieces_) {
     N = N_;
     mmax = mmax_;
     pieces = pieces_;
-    const size_t elems = (size_t)N * mmax;
-    QG_TRY(split_a.reserve((size_t)pieces * elems * sizeof(__nv_bfloat16)));
-    QG_TRY(split_b.reserve((size_t)pieces * elems * sizeof(__nv_bfloat16)));
-    return QG_OK;
+    QG_TRY(split_a.reserve((size_t)pieces * N * mmax * sizeof(__nv_bfloat16)));
+    return QG_OK;  // the B-side slot is allocated by the first split into it
 }
 
 int TcGram::split(const double* A, int m, int which, cudaStream_t st) {
     DevBuf& b = which == 0 ? split_a : split_b;
+    QG_TRY(b.reserve((size_t)pieces * N * mmax * sizeof(__nv_bfloat16)));
     const long long n = N * m;
     const long long ps = N * mmax;
     if (pieces == 2)

@@ -32,7 +32,11 @@ struct qg_context_s {
     void* solver = nullptr;    // cusolverDnHandle_t, created on first use
     int live_hamiltonians = 0; // the context outlives every operator built on it
     int* dev_status = nullptr; // device status word set by kernels whose bounded waits gave up
+    void* gram_cache = nullptr; // qg::MixedGram buffers kept by qg_gram_mixed_d across calls
 };
+
+// Frees the context's qg_gram_mixed_d buffers (gram_mixed.cu).
+void qg_release_gram_cache(qg_context c);
 
 // A device buffer that only grows.
 struct DevBuf {
