@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     p.add_argument("--no-kpoint", action="store_true", help="skip the k-point leg (64 Monkhorst-Pack points)")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-preconditioner leg (GPU training and an unseen-cell comparison)")
     p.add_argument("--only", choices=["kpoint", "gram"], default=None,
                    help="run one leg alone and print its JSON (profiling captures)")
     p.add_argument("--kpoints", type=int, default=64, help="k-points of the k-point leg (4x4x4 grid order)")
@@ -349,6 +351,32 @@ def kpoint_leg(ctx, n_k=64, steps=10):
     return {"workload": "diamond8_40cube_16states_mp4x4x4_fd8_complex", "apply": apply, "lobpcg": solves}
 
 
+def learned_leg(ctx, steps=1500):
+    """Learned preconditioner: (residual, correction) pairs from LOBPCG iterates on four
+    8-atom 40^3 cells, GPU training with the engine's own forward/backward kernels, then
+    LOBPCG with the kinetic preconditioner against kinetic + learned correction on an
+    unseen 8-atom cell (atoms displaced by sigma 0.1 bohr), 16 states, 14 converged."""
+    from qumasun_b200 import learned as LP
+    from qumasun_b200.cell import build_cell
+    t0 = time.perf_counter()
+    data = []
+    for i, c in enumerate(LP.default_training_cells()):
+        R, Cc, V = LP.residual_pairs(ctx, c, 16, (2, 4, 7, 11, 16), seed=100 + i)
+        data.append(((c.nx, c.ny, c.nz), R, Cc, V))
+    t1 = time.perf_counter()
+    nn, hist = LP.train(ctx, data, steps=steps, log_every=max(1, steps // 5))
+    t2 = time.perf_counter()
+    hc = build_cell(displacement=0.1, seed=99)
+    Rh, Ch, Vh = LP.residual_pairs(ctx, hc, 16, (3, 8), seed=77)
+    held = LP.held_out_loss(nn, [((hc.nx, hc.ny, hc.nz), Rh, Ch, Vh)])
+    cmp = LP.compare(ctx, nn, build_cell(displacement=0.1, seed=98), 16, n_converge=14)
+    nn.close()
+    return {"workload": "diamond8_40cube_train4cells_eval_unseen_sigma0.1", "pairs": sum(d[1].shape[0] for d in data),
+            "pair_generation_s": round(t1 - t0, 2), "training_steps": steps, "training_s": round(t2 - t1, 2),
+            "loss_history": [[s_, round(l_, 4)] for s_, l_ in hist], "held_out_loss": round(held, 4),
+            "lobpcg_unseen_cell": cmp}
+
+
 def lobpcg_diamond216(ctx):
     """Time to the 480 lowest eigenpairs (528 solved, a 48-state guard band) of the
     216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
@@ -520,6 +548,9 @@ def run_gpu_arm(a):
     kp = None
     if rank == 0 and not a.no_kpoint:
         kp = kpoint_leg(ctx, n_k=a.kpoints)
+    lrn = None
+    if rank == 0 and not a.no_learned:
+        lrn = learned_leg(ctx)
     lob = None
     lob216 = None
     if rank == 0 and not a.no_lobpcg:
@@ -561,6 +592,8 @@ def run_gpu_arm(a):
             line["lobpcg_216"] = lob216
         if kp:
             line["kpoint"] = kp
+        if lrn:
+            line["learned_preconditioner"] = lrn
         print(json.dumps(line), flush=True)
     H.close()
     ctx.close()

@@ -37,11 +37,13 @@ typedef enum qg_status {
     QG_ERR_NOT_CONVERGED = -9  /* solver hit its iteration limit (results still written) */
 } qg_status;
 
-/* QG_MIXED_BF16X3 (LOBPCG only): the Gram products run as split-BF16x3 tensor-core
- * GEMMs with FP32 accumulation (FP64 across 1024-row K chunks) until the residual
- * falls below 1e-6 or stops halving, then as FP64; H, residuals, rotations, norms
- * and the small eigensolves stay FP64 throughout (a solve that ends while still
- * mixed takes a final FP64 Rayleigh-Ritz on X). */
+/* QG_MIXED_BF16X3 (LOBPCG only): the Gram products run on the library's tcgen05
+ * kernel with every FP64 value split into 3 bfloat16 pieces (6 products, FP32
+ * accumulation over one 64-row K block, FP64 across blocks; rows not a multiple of
+ * 8 use cuBLAS BF16 GEMMs on 2 pieces) until the residual falls below 1e-6 or stops
+ * halving, then as FP64; H, residuals, rotations, norms and the small eigensolves
+ * stay FP64 throughout (a solve that reaches the tolerance or max_iter while still
+ * mixed takes an FP64 Rayleigh-Ritz on X before its residuals are judged). */
 typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2 } qg_precision;
 
 typedef struct qg_context_s* qg_context;
@@ -184,7 +186,8 @@ typedef struct qg_lobpcg_options {
     int precision;      /* QG_FP64: FP64 throughout; QG_MIXED_BF16X3: split-BF16x3 Gram products */
     int verbose;        /* 1: print (iteration, max residual) lines to stdout */
     int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
-                           applied in Fourier space with the FD stencil's own symbol */
+                           applied in Fourier space with the FD stencil's own symbol; 2: kinetic
+                           plus the learned correction of qg_hamiltonian_set_learned */
     double precond_shift; /* shift (Ha) of the kinetic preconditioner; <= 0 selects 1.0 */
     int n_converge;     /* the lowest n_converge states must meet tol, the others are a guard
                            band against a degenerate multiplet at the cut; <= 0 or >= ns: all */
