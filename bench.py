@@ -292,62 +292,77 @@ def monkhorst_pack(n, a0):
     return [(b * fx, b * fy, b * fz) for fz in f for fy in f for fx in f]
 
 
-def kpoint_leg(ctx, n_k=64, steps=10):
+def kpoint_leg(ctx, n_k=64, steps=10, rank=0, ws=1):
     """Complex k-point operator on the 8-atom 40^3 cell, 16 states per k-point, over a
-    4x4x4 Monkhorst-Pack grid: (1) H_k|psi> throughput of the complex apply, (2) time to
-    the 16 lowest eigenpairs at every k-point (FP64 complex LOBPCG, kinetic
-    preconditioner, k-points one after another through qg_hamiltonian_set_kvector)."""
+    4x4x4 Monkhorst-Pack grid: (1) H_k|psi> throughput of the complex apply (rank 0),
+    (2) time to the 16 lowest eigenpairs at every k-point (FP64 complex LOBPCG, kinetic
+    preconditioner). With several ranks the k-points are sharded by longest-processing-
+    time assignment (qumasun_b200.shard), one GPU per rank, no collective on the data
+    path; the time is the max over ranks and rank 0 gathers the eigenvalues."""
     import numpy as np
     import torch
     from qumasun_b200 import Hamiltonian
-    from qumasun_b200.cell import build_cell
+    from qumasun_b200.cell import build_cell, initial_states
+    from qumasun_b200.shard import run_sharded
     cell = build_cell()
     N, ns = cell.N, 16
     mp = monkhorst_pack(4, 6.74)
     ks = mp[:n_k]
     H = Hamiltonian(ctx, cell, kvec=mp[0])
-    gen = torch.Generator(device="cuda").manual_seed(77)
-    X = torch.rand(ns, 2 * N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
-    HX = torch.empty_like(X)
-    for _ in range(3):
-        H.apply_z(X, HX)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        H.apply_z(X, HX)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    phases = sorted((H.apply_timed_z(ns, X.data_ptr(), HX.data_ptr()) for _ in range(5)), key=lambda p: p[1])[2]
-    nbytes = N * ns * 32 + N * 8
-    apply = {"ms": round(ms, 4), "GBs": round(nbytes / (ms * 1e-3) / 1e9, 1),
-             "state_apps_per_s": round(ns / (ms * 1e-3), 1),
-             "phase_ms": {"projection": round(phases[0], 4), "stencil_V": round(phases[1], 4),
-                          "scatter": round(phases[2], 4)}}
+    apply = None
+    if rank == 0:
+        gen = torch.Generator(device="cuda").manual_seed(77)
+        X = torch.rand(ns, 2 * N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+        HX = torch.empty_like(X)
+        for _ in range(3):
+            H.apply_z(X, HX)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            H.apply_z(X, HX)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        phases = sorted((H.apply_timed_z(ns, X.data_ptr(), HX.data_ptr()) for _ in range(5)), key=lambda p: p[1])[2]
+        nbytes = N * ns * 32 + N * 8
+        apply = {"ms": round(ms, 4), "GBs": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                 "state_apps_per_s": round(ns / (ms * 1e-3), 1),
+                 "phase_ms": {"projection": round(phases[0], 4), "stencil_V": round(phases[1], 4),
+                              "scatter": round(phases[2], 4)}}
+        del X, HX
     solves = None
     if n_k > 0:
-        from qumasun_b200.cell import initial_states
         X0 = initial_states(ns, 2 * N, seed=1234)
-        evs, its = [], []
+
+        def solve(i):
+            H.set_kvector(ks[i])
+            r = H.lobpcg_z(X0, max_iter=500, precond=1, tol=1e-10)
+            return {"ev": r["ev"].tolist(), "iterations": r["report"]["iterations"],
+                    "device_ms": r["report"]["ms_total"]}
+
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dev_ms = 0.0
-        for k in ks:
-            H.set_kvector(k)
-            r = H.lobpcg_z(X0, max_iter=500, precond=1, tol=1e-10)
-            evs.append(r["ev"])
-            its.append(r["report"]["iterations"])
-            dev_ms += r["report"]["ms_total"]
+        res = run_sharded([1.0] * n_k, solve)
         wall = time.perf_counter() - t0
-        evs = np.array(evs)
-        # time reversal: E(k) = E(-k); the Monkhorst-Pack grid holds both of each pair
-        pair = float(max(np.abs(np.sort(evs[i]) - np.sort(evs[n_k - 1 - i])).max() for i in range(n_k)))
-        solves = {"k_points": n_k, "states_per_k": ns, "seconds": round(wall, 3), "device_ms": round(dev_ms, 1),
-                  "iterations_max": int(max(its)), "iterations_mean": round(float(np.mean(its)), 1),
-                  "band_min_Ha": float(evs.min()), "band_max_Ha": float(evs.max()),
-                  "max_abs_ev_diff_k_vs_minus_k_Ha": pair}
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        if rank == 0:
+            evs = np.array([res[i]["ev"] for i in range(n_k)])
+            its = [res[i]["iterations"] for i in range(n_k)]
+            # time reversal: E(k) = E(-k); the Monkhorst-Pack grid holds both of each pair
+            pair = float(max(np.abs(np.sort(evs[i]) - np.sort(evs[n_k - 1 - i])).max() for i in range(n_k)))
+            solves = {"k_points": n_k, "states_per_k": ns, "ranks": ws, "seconds": round(wall, 3),
+                      "device_ms": round(sum(res[i]["device_ms"] for i in range(n_k)), 1),
+                      "iterations_max": int(max(its)), "iterations_mean": round(float(np.mean(its)), 1),
+                      "band_min_Ha": float(evs.min()), "band_max_Ha": float(evs.max()),
+                      "max_abs_ev_diff_k_vs_minus_k_Ha": pair}
     H.close()
+    if rank != 0:
+        return None
     return {"workload": "diamond8_40cube_16states_mp4x4x4_fd8_complex", "apply": apply, "lobpcg": solves}
 
 
@@ -546,8 +561,8 @@ def run_gpu_arm(a):
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
     kp = None
-    if rank == 0 and not a.no_kpoint:
-        kp = kpoint_leg(ctx, n_k=a.kpoints)
+    if not a.no_kpoint:
+        kp = kpoint_leg(ctx, n_k=a.kpoints, rank=rank, ws=ws)
     lrn = None
     if rank == 0 and not a.no_learned:
         lrn = learned_leg(ctx)
