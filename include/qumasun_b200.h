@@ -144,6 +144,15 @@ int qg_hamiltonian_apply_host_d(qg_hamiltonian ham, int ns, const double* X, dou
  * (GridDifferenceKpoint8th.h:325-368). */
 int qg_hamiltonian_apply_z(qg_hamiltonian ham, int ns, const double* X, long long ldx,
                            double* HX, long long ldhx);
+/* The k-point operator for nk k-points in one pass: kvecs = nk Bloch vectors (HOST,
+ * 3 doubles each, bohr^-1), nsk states per k-point, state s of k-point k at
+ * X + k*ldk + s*ldx (HX + k*ldkh + s*ldhx), DEVICE FP64, ldx/ldhx >= 2N,
+ * ldk >= nsk*ldx. Each stencil work item and projector block carries its k-point's
+ * coefficients and Bloch tables, so all k-points share one launch per phase. The
+ * operator's own k-vector (qg_hamiltonian_set_kvector) is not used. No counterpart in
+ * the reference, which loops over k (qumasun_kpoint.lobpcg.h:25-41). */
+int qg_hamiltonian_apply_zk(qg_hamiltonian ham, int nk, const double* kvecs, int nsk, const double* X,
+                            long long ldx, long long ldk, double* HX, long long ldhx, long long ldkh);
 /* qg_hamiltonian_apply_z with HOST buffers (ns * 2N doubles each, ldx = 2N). */
 int qg_hamiltonian_apply_host_z(qg_hamiltonian ham, int ns, const double* X, double* HX);
 /* qg_hamiltonian_apply_z with the phase timing of qg_hamiltonian_apply_timed_d. */

@@ -501,7 +501,7 @@ void free_projectors(DevProjectors& pj) {
     cudaFree(pj.atom_off); cudaFree(pj.pt_g); cudaFree(pj.tab_d); cudaFree(pj.tab_f);
     cudaFree(pj.ch_scale); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
     cudaFree(pj.ent_val_f); cudaFree(pj.pt_u); cudaFree(pj.ent_pt); cudaFree(pj.ztab); cudaFree(pj.zent);
-    pj = DevProjectors{};
+    pj = DevProjectors();
 }
 
 // Compacts the reference's per-atom cube tables into sphere point lists and the
@@ -621,6 +621,7 @@ void destroy_ham(qg_hamiltonian h) {
     cudaFree(h->V_f);
     free_projectors(h->pj);
     h->coef.release();
+    h->kco.release();
     h->xio.release();
     h->hxio.release();
     delete h;

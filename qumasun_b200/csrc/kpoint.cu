@@ -49,17 +49,21 @@ __global__ void k_bloch_tables(const double* __restrict__ tab, const int* __rest
     }
 }
 
-// Complex gather-contraction: one block per (atom, group of SB states).
-// c = sum_p (tr + i ti)(ur + i ui), scaled by E dV per channel.
+// Complex gather-contraction: one block per (atom, k-point, group of SB states).
+// c = sum_p (tr + i ti)(ur + i ui), scaled by E dV per channel; the states of k-point k
+// start at X + k*ldk, the Bloch tables of k at ztab + k*zstride.
 template <int SB, int NCH>
-__global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X, long long ldx, long long xim, int ns,
+__global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X, long long ldx, long long ldk,
+                                                   long long xim, int nsk, int groups,
                                                    const int* __restrict__ atom_off, const int* __restrict__ pt_g,
-                                                   const double* __restrict__ ztab, long long npts,
+                                                   const double* __restrict__ ztab, long long zstride, long long npts,
                                                    const double* __restrict__ ch_scale, double* __restrict__ coef,
                                                    int ncoef) {
     const int atom = blockIdx.x;
-    const int s0 = blockIdx.y * SB;
+    const int k = blockIdx.y / groups;
+    const int s0 = (blockIdx.y - k * groups) * SB;
     const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
+    const double* tab = ztab + (long long)k * zstride;
     double ar[SB][NCH], ai[SB][NCH];
 #pragma unroll
     for (int s = 0; s < SB; ++s)
@@ -67,15 +71,15 @@ __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X,
         for (int c = 0; c < NCH; ++c) ar[s][c] = ai[s][c] = 0.0;
     const double* Xs[SB];
 #pragma unroll
-    for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
+    for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)k * ldk + (long long)min(s0 + s, nsk - 1) * ldx;
 
     for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const int g = pt_g[p];
         double tr[NCH], ti[NCH];
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
-            tr[c] = ztab[(long long)c * npts + p];
-            ti[c] = ztab[(long long)(NCH + c) * npts + p];
+            tr[c] = tab[(long long)c * npts + p];
+            ti[c] = tab[(long long)(NCH + c) * npts + p];
         }
 #pragma unroll
         for (int s = 0; s < SB; ++s) {
@@ -110,55 +114,60 @@ __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X,
         double v = 0.0;
         for (int w = 0; w < nw; ++w) v += red[w][i];
         const int sc = i >> 1, s = sc / NCH, c = sc % NCH;
-        if (s0 + s < ns) coef[((long long)(s0 + s) * ncoef + atom * NCH + c) * 2 + (i & 1)] = ch_scale[atom * NCH + c] * v;
+        if (s0 + s < nsk)
+            coef[(((long long)k * nsk + s0 + s) * ncoef + atom * NCH + c) * 2 + (i & 1)] = ch_scale[atom * NCH + c] * v;
     }
 }
 
-// Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[s][a_e, ch].
+// Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[s][a_e, ch],
+// k-point by k-point (tables zent + k*zstride, states of k at HX + k*ldk).
 template <int SG, int NCH>
-__global__ void __launch_bounds__(256) k_scatter_all_z(double* __restrict__ HX, long long ldhx, long long hxim, int ns,
-                                                       long long N, const int* __restrict__ row,
-                                                       const int* __restrict__ ent_atom,
-                                                       const double* __restrict__ zent,
+__global__ void __launch_bounds__(256) k_scatter_all_z(double* __restrict__ HX, long long ldhx, long long ldk,
+                                                       long long hxim, int nk, int nsk, long long N,
+                                                       const int* __restrict__ row, const int* __restrict__ ent_atom,
+                                                       const double* __restrict__ zent, long long zstride,
                                                        const double* __restrict__ coef, int ncoef) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= N) return;
     const int e0 = row[g], e1 = row[g + 1];
     if (e0 == e1) return;
-    for (int s0 = 0; s0 < ns; s0 += SG) {
-        const int gn = min(SG, ns - s0);
-        double accr[SG], acci[SG];
+    for (int k = 0; k < nk; ++k) {
+        const double* zk = zent + (long long)k * zstride;
+        for (int s0 = 0; s0 < nsk; s0 += SG) {
+            const int gn = min(SG, nsk - s0);
+            double accr[SG], acci[SG];
 #pragma unroll
-        for (int s = 0; s < SG; ++s) accr[s] = acci[s] = 0.0;
-        const double* cg = coef + (long long)s0 * ncoef * 2;
-        for (int e = e0; e < e1; ++e) {
-            const int base = __ldg(&ent_atom[e]) * NCH;
-            double vr[NCH], vi[NCH];
+            for (int s = 0; s < SG; ++s) accr[s] = acci[s] = 0.0;
+            const double* cg = coef + ((long long)k * nsk + s0) * ncoef * 2;
+            for (int e = e0; e < e1; ++e) {
+                const int base = __ldg(&ent_atom[e]) * NCH;
+                double vr[NCH], vi[NCH];
 #pragma unroll
-            for (int c = 0; c < NCH; ++c) {
-                vr[c] = __ldg(&zent[((long long)e * NCH + c) * 2]);
-                vi[c] = __ldg(&zent[((long long)e * NCH + c) * 2 + 1]);
-            }
+                for (int c = 0; c < NCH; ++c) {
+                    vr[c] = __ldg(&zk[((long long)e * NCH + c) * 2]);
+                    vi[c] = __ldg(&zk[((long long)e * NCH + c) * 2 + 1]);
+                }
 #pragma unroll
-            for (int s = 0; s < SG; ++s) {
-                if (s < gn) {
+                for (int s = 0; s < SG; ++s) {
+                    if (s < gn) {
 #pragma unroll
-                    for (int c = 0; c < NCH; ++c) {
-                        const double cr = __ldg(&cg[((long long)s * ncoef + base + c) * 2]);
-                        const double ci = __ldg(&cg[((long long)s * ncoef + base + c) * 2 + 1]);
-                        accr[s] += vr[c] * cr + vi[c] * ci;
-                        acci[s] += vr[c] * ci - vi[c] * cr;
+                        for (int c = 0; c < NCH; ++c) {
+                            const double cr = __ldg(&cg[((long long)s * ncoef + base + c) * 2]);
+                            const double ci = __ldg(&cg[((long long)s * ncoef + base + c) * 2 + 1]);
+                            accr[s] += vr[c] * cr + vi[c] * ci;
+                            acci[s] += vr[c] * ci - vi[c] * cr;
+                        }
                     }
                 }
             }
-        }
 #pragma unroll
-        for (int s = 0; s < SG; ++s)
-            if (s < gn) {
-                double* hr = HX + (long long)(s0 + s) * ldhx + g;
-                hr[0] += accr[s];
-                hr[hxim] += acci[s];
-            }
+            for (int s = 0; s < SG; ++s)
+                if (s < gn) {
+                    double* hr = HX + (long long)k * ldk + (long long)(s0 + s) * ldhx + g;
+                    hr[0] += accr[s];
+                    hr[hxim] += acci[s];
+                }
+        }
     }
 }
 
@@ -170,9 +179,24 @@ __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<double> a) {
     if (i >= N) return;
     const int s = blockIdx.y;
     const int ix = (int)(i % a.nx), iy = (int)((i / a.nx) % a.ny), iz = (int)(i / ((long long)a.nx * a.ny));
+    double c0 = a.c0, dxc[4], dyc[4], dzc[4];
+    for (int d = 0; d < 4; ++d) {
+        dxc[d] = a.dx[d];
+        dyc[d] = a.dy[d];
+        dzc[d] = a.dz[d];
+    }
+    if (a.kco) {
+        const double* kc = a.kco + (long long)(s / a.nsk) * 13;
+        c0 = kc[0];
+        for (int d = 0; d < 4; ++d) {
+            dxc[d] = kc[1 + d];
+            dyc[d] = kc[5 + d];
+            dzc[d] = kc[9 + d];
+        }
+    }
     double lap[2], der[2], cen[2];
     for (int c = 0; c < 2; ++c) {
-        const double* u = a.X + (long long)s * a.ldx + (c ? a.xim : 0);
+        const double* u = a.X + state_offset(a, s, false) + (c ? a.xim : 0);
         auto at = [&](int dx, int dy, int dz) {
             return u[wrap_idx(ix + dx, a.nx) + (long long)a.nx * (wrap_idx(iy + dy, a.ny) + (long long)a.ny * wrap_idx(iz + dz, a.nz))];
         };
@@ -183,114 +207,149 @@ __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<double> a) {
             zm[d - 1] = at(0, 0, -d); zp[d - 1] = at(0, 0, d);
         }
         cen[c] = u[i];
-        double l = a.c0 * cen[c];
+        double l = c0 * cen[c];
         l += a.cx[3] * (xp[3] + xm[3]) + a.cx[2] * (xp[2] + xm[2]) + a.cx[1] * (xp[1] + xm[1]) + a.cx[0] * (xp[0] + xm[0]);
         l += a.cy[3] * (yp[3] + ym[3]) + a.cy[2] * (yp[2] + ym[2]) + a.cy[1] * (yp[1] + ym[1]) + a.cy[0] * (yp[0] + ym[0]);
         l += a.cz[3] * (zp[3] + zm[3]) + a.cz[2] * (zp[2] + zm[2]) + a.cz[1] * (zp[1] + zm[1]) + a.cz[0] * (zp[0] + zm[0]);
         lap[c] = l;
-        double g = a.dx[3] * (xp[3] - xm[3]) + a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
-        g += a.dy[3] * (yp[3] - ym[3]) + a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
-        g += a.dz[3] * (zp[3] - zm[3]) + a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
+        double g = dxc[3] * (xp[3] - xm[3]) + dxc[2] * (xp[2] - xm[2]) + dxc[1] * (xp[1] - xm[1]) + dxc[0] * (xp[0] - xm[0]);
+        g += dyc[3] * (yp[3] - ym[3]) + dyc[2] * (yp[2] - ym[2]) + dyc[1] * (yp[1] - ym[1]) + dyc[0] * (yp[0] - ym[0]);
+        g += dzc[3] * (zp[3] - zm[3]) + dzc[2] * (zp[2] - zm[2]) + dzc[1] * (zp[1] - zm[1]) + dzc[0] * (zp[0] - zm[0]);
         der[c] = g;
     }
     const double v = a.V[i];
-    double* h = a.HX + (long long)s * a.ldhx + i;
+    double* h = a.HX + state_offset(a, s, true) + i;
     h[0] = (v * cen[0] + lap[0]) - der[1];
     h[a.hxim] = (v * cen[1] + lap[1]) + der[0];
 }
 
 template <int NCH>
-void launch_project_z_nch(const DevProjectors& pj, int ns, const double* X, long long ldx, long long xim,
-                          double* coef, cudaStream_t st) {
-    if (pj.na * ((ns + 3) / 4) >= 2 * 148) {
-        dim3 g(pj.na, (ns + 3) / 4);
-        k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
-                                               coef, pj.na * NCH);
-    } else if (pj.na * ((ns + 1) / 2) >= 2 * 148) {
-        dim3 g(pj.na, (ns + 1) / 2);
-        k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
-                                               coef, pj.na * NCH);
+void launch_project_z_nch(const DevProjectors& pj, int nk, int nsk, const double* X, long long ldx, long long ldk,
+                          long long xim, double* coef, cudaStream_t st) {
+    const long long zstride = 2LL * pj.nch * pj.npts;
+    if (pj.na * nk * ((nsk + 3) / 4) >= 2 * 148) {
+        const int groups = (nsk + 3) / 4;
+        dim3 g(pj.na, nk * groups);
+        k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
+                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
+    } else if (pj.na * nk * ((nsk + 1) / 2) >= 2 * 148) {
+        const int groups = (nsk + 1) / 2;
+        dim3 g(pj.na, nk * groups);
+        k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
+                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
     } else {
-        dim3 g(pj.na, ns);
-        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, xim, ns, pj.atom_off, pj.pt_g, pj.ztab, pj.npts, pj.ch_scale,
-                                               coef, pj.na * NCH);
+        dim3 g(pj.na, nk * nsk);
+        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, nsk, pj.atom_off, pj.pt_g, pj.ztab, zstride,
+                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
     }
 }
 
 template <int NCH>
-void launch_scatter_z_nch(const DevProjectors& pj, double* HX, long long ldhx, long long hxim, int ns, long long N,
-                          const double* coef, cudaStream_t st) {
-    k_scatter_all_z<4, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(HX, ldhx, hxim, ns, N, pj.row, pj.ent_atom,
-                                                                         pj.zent, coef, pj.na * NCH);
+void launch_scatter_z_nch(const DevProjectors& pj, int nk, int nsk, double* HX, long long ldhx, long long ldk,
+                          long long hxim, long long N, const double* coef, cudaStream_t st) {
+    k_scatter_all_z<4, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        HX, ldhx, ldk, hxim, nk, nsk, N, pj.row, pj.ent_atom, pj.zent, 2LL * pj.nch * pj.nent, coef, pj.na * NCH);
 }
 
-// Bloch-phase tables for the operator's current k-vector.
-int ensure_bloch_tables(qg_hamiltonian h, cudaStream_t st) {
+// Bloch-phase tables for the k-vectors kv (3 per k-point), rebuilt when they change.
+int ensure_bloch_tables(qg_hamiltonian h, int nk, const double* kv, cudaStream_t st) {
     DevProjectors& pj = h->pj;
     if (pj.na <= 0 || pj.nch <= 0) return QG_OK;
-    if (pj.zready && pj.zg[0] == h->gx && pj.zg[1] == h->gy && pj.zg[2] == h->gz) return QG_OK;
-    if (!pj.ztab) {
-        QG_CUDA_TRY(cudaMalloc(&pj.ztab, (size_t)2 * pj.nch * pj.npts * sizeof(double)));
-        QG_CUDA_TRY(cudaMalloc(&pj.zent, (size_t)2 * pj.nch * pj.nent * sizeof(double)));
+    if (pj.zready && (int)pj.zk.size() == 3 * nk && std::equal(kv, kv + 3 * nk, pj.zk.begin())) return QG_OK;
+    const size_t tab = (size_t)2 * pj.nch * pj.npts, ent = (size_t)2 * pj.nch * pj.nent;
+    if (nk > pj.zcap) {
+        cudaFree(pj.ztab);
+        cudaFree(pj.zent);
+        pj.ztab = pj.zent = nullptr;
+        pj.zcap = 0;
+        QG_CUDA_TRY(cudaMalloc(&pj.ztab, tab * nk * sizeof(double)));
+        QG_CUDA_TRY(cudaMalloc(&pj.zent, ent * nk * sizeof(double)));
+        pj.zcap = nk;
     }
     const long long total = pj.npts + pj.nent;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    k_bloch_tables<<<blocks, 256, 0, st>>>(pj.tab_d, pj.pt_u, pj.npts, pj.ent_pt, pj.nent, pj.nch, h->gx * h->hx,
-                                           h->gy * h->hy, h->gz * h->hz, pj.ztab, pj.zent);
+    for (int k = 0; k < nk; ++k)
+        k_bloch_tables<<<blocks, 256, 0, st>>>(pj.tab_d, pj.pt_u, pj.npts, pj.ent_pt, pj.nent, pj.nch,
+                                               kv[3 * k] * h->hx, kv[3 * k + 1] * h->hy, kv[3 * k + 2] * h->hz,
+                                               pj.ztab + tab * k, pj.zent + ent * k);
     QG_CUDA_TRY(cudaGetLastError());
-    pj.zg[0] = h->gx; pj.zg[1] = h->gy; pj.zg[2] = h->gz;
+    pj.zk.assign(kv, kv + 3 * nk);
     pj.zready = true;
     return QG_OK;
 }
 
+// c0 and the first-derivative coefficients of -1/2 (Lap + 2i g.grad - g^2), exactly as
+// LaplasianKpoint8th_halo_f forms them: out[0] = c0, out[1..4] = dx, [5..8] = dy, [9..12] = dz
+void kpoint_coefs(const qg_hamiltonian h, const double* g, double* out) {
+    const double coefk = -0.5;
+    const double hh[3] = {h->hx, h->hy, h->hz};
+    out[0] = -14350.0 / 5040.0 * coefk * (1.0 / (hh[0] * hh[0]) + 1.0 / (hh[1] * hh[1]) + 1.0 / (hh[2] * hh[2])) -
+             coefk * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    const double coef2 = coefk * 2.0;
+    for (int d = 0; d < 3; ++d) {
+        const bool on = std::fabs(g[d]) >= 1.0e-8;  // LaplasianKpoint8th_ddm skips |g| < 1e-8
+        double* o = out + 1 + 4 * d;
+        o[0] = on ? 672.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
+        o[1] = on ? -168.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
+        o[2] = on ? 32.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
+        o[3] = on ? -3.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
+    }
+}
+
 }  // namespace
 
-int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
-                        double* coef, cudaStream_t st, PhaseTimer* pt) {
+int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, const double* X, long long ldx,
+                         long long ldk, double* HX, long long ldhx, long long ldkh, double* coef, cudaStream_t st,
+                         PhaseTimer* pt) {
     if (h->order != 8) return QG_ERR_UNSUPPORTED;
     const DevProjectors& pj = h->pj;
     const long long N = h->N();
     HamArgs<double> a{};
-    a.X = X; a.ldx = ldx; a.HX = HX; a.ldhx = ldhx; a.ns = ns;
+    a.X = X; a.ldx = ldx; a.HX = HX; a.ldhx = ldhx; a.ns = nk * nsk;
     a.xim = N; a.hxim = N;
     a.V = h->V_d;
     a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.ty = h->ty;
     a.err = h->ctx->dev_status;
-    // -1/2 (Lap + 2i g.grad - g^2) exactly as LaplasianKpoint8th_halo_f forms it
     const double coefk = -0.5;
     const double hh[3] = {h->hx, h->hy, h->hz};
-    const double gg[3] = {h->gx, h->gy, h->gz};
     double* cs[3] = {a.cx, a.cy, a.cz};
-    double* ds[3] = {a.dx, a.dy, a.dz};
-    a.c0 = -14350.0 / 5040.0 * coefk * (1.0 / (hh[0] * hh[0]) + 1.0 / (hh[1] * hh[1]) + 1.0 / (hh[2] * hh[2])) -
-           coefk * (gg[0] * gg[0] + gg[1] * gg[1] + gg[2] * gg[2]);
-    const double coef2 = coefk * 2.0;
     for (int d = 0; d < 3; ++d) {
         const double s = 5040.0 * hh[d] * hh[d];
         cs[d][3] = -9.0 * coefk / s;
         cs[d][2] = 128.0 * coefk / s;
         cs[d][1] = -1008.0 * coefk / s;
         cs[d][0] = 8064.0 * coefk / s;
-        const bool on = std::fabs(gg[d]) >= 1.0e-8;  // LaplasianKpoint8th_ddm skips |g| < 1e-8
-        ds[d][0] = on ? 672.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
-        ds[d][1] = on ? -168.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
-        ds[d][2] = on ? 32.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
-        ds[d][3] = on ? -3.0 * coef2 * gg[d] / (840.0 * hh[d]) : 0.0;
+    }
+    std::vector<double> kc((size_t)13 * nk);
+    for (int k = 0; k < nk; ++k) kpoint_coefs(h, kv + 3 * k, kc.data() + 13 * k);
+    a.c0 = kc[0];
+    for (int d = 0; d < 4; ++d) {
+        a.dx[d] = kc[1 + d];
+        a.dy[d] = kc[5 + d];
+        a.dz[d] = kc[9 + d];
+    }
+    if (nk > 1) {
+        QG_TRY(h->kco.reserve(kc.size() * sizeof(double)));
+        QG_CUDA_TRY(cudaMemcpyAsync(h->kco.ptr, kc.data(), kc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        a.kco = h->kco.as<double>();
+        a.nsk = nsk;
+        a.ldkx = ldk;
+        a.ldkhx = ldkh;
     }
     const bool nonlocal = pj.na > 0 && pj.nch > 0;
     if (pt) pt->mark(0, st);
     if (nonlocal) {
-        QG_TRY(ensure_bloch_tables(h, st));
+        QG_TRY(ensure_bloch_tables(h, nk, kv, st));
         switch (pj.nch) {
-            case 4: launch_project_z_nch<4>(pj, ns, X, ldx, N, coef, st); break;
-            case 8: launch_project_z_nch<8>(pj, ns, X, ldx, N, coef, st); break;
-            case 16: launch_project_z_nch<16>(pj, ns, X, ldx, N, coef, st); break;
+            case 4: launch_project_z_nch<4>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
+            case 8: launch_project_z_nch<8>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
+            case 16: launch_project_z_nch<16>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
             default: return QG_ERR_UNSUPPORTED;
         }
     }
     if (pt) pt->mark(1, st);
-    if (h->force_plain_stencil || !stencil_tma_ok<double>(a, 8, 2)) {
-        dim3 g((unsigned)((N + 255) / 256), (unsigned)ns);
+    if (h->force_plain_stencil || !stencil_tma_ok<double>(a, 8, 2) || (nk > 1 && (ldk % 2 || ldkh % 2))) {
+        dim3 g((unsigned)((N + 255) / 256), (unsigned)(nk * nsk));
         k_kpoint_plain<<<g, 256, 0, st>>>(a);
     } else {
         QG_TRY(launch_stencil_tma<double>(a, 8, st, 2));
@@ -298,14 +357,20 @@ int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx
     if (pt) pt->mark(2, st);
     if (nonlocal) {
         switch (pj.nch) {
-            case 4: launch_scatter_z_nch<4>(pj, HX, ldhx, N, ns, N, coef, st); break;
-            case 8: launch_scatter_z_nch<8>(pj, HX, ldhx, N, ns, N, coef, st); break;
-            default: launch_scatter_z_nch<16>(pj, HX, ldhx, N, ns, N, coef, st); break;
+            case 4: launch_scatter_z_nch<4>(pj, nk, nsk, HX, ldhx, ldkh, N, N, coef, st); break;
+            case 8: launch_scatter_z_nch<8>(pj, nk, nsk, HX, ldhx, ldkh, N, N, coef, st); break;
+            default: launch_scatter_z_nch<16>(pj, nk, nsk, HX, ldhx, ldkh, N, N, coef, st); break;
         }
     }
     if (pt) pt->mark(-1, st);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
+}
+
+int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
+                        double* coef, cudaStream_t st, PhaseTimer* pt) {
+    const double kv[3] = {h->gx, h->gy, h->gz};
+    return apply_hamiltonian_zk(h, 1, kv, ns, X, ldx, 0, HX, ldhx, 0, coef, st, pt);
 }
 
 }  // namespace qg
@@ -330,6 +395,23 @@ int apply_z_checked(qg_hamiltonian h, int ns, const double* X, long long ldx, do
 }  // namespace
 
 extern "C" {
+
+int qg_hamiltonian_apply_zk(qg_hamiltonian h, int nk, const double* kvecs, int nsk, const double* X, long long ldx,
+                            long long ldk, double* HX, long long ldhx, long long ldkh) {
+    if (!h || nk <= 0 || nsk < 0 || !kvecs || (nsk > 0 && (!X || !HX))) return QG_ERR_INVALID;
+    if (nsk == 0) return QG_OK;
+    const long long N = h->N();
+    if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
+    if (nk > 1 && (ldk < (long long)nsk * ldx || ldkh < (long long)nsk * ldhx)) return QG_ERR_INVALID;
+    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    double* coef = nullptr;
+    if (h->pj.na > 0) {
+        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, nk * nsk) * sizeof(double)));
+        coef = h->coef.as<double>();
+    }
+    return qg::apply_hamiltonian_zk(h, nk, kvecs, nsk, X, ldx, ldk, HX, ldhx, ldkh, coef, h->ctx->stream);
+}
 
 int qg_hamiltonian_apply_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx) {
     return apply_z_checked(h, ns, X, ldx, HX, ldhx);

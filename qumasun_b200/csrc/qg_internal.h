@@ -87,7 +87,8 @@ struct DevProjectors {
     int* ent_pt = nullptr;
     double* ztab = nullptr;
     double* zent = nullptr;
-    double zg[3] = {0, 0, 0};
+    std::vector<double> zk;  // k-vectors (3 per k-point) the tables were built for
+    int zcap = 0;            // k-points the table buffers hold
     bool zready = false;
 };
 
@@ -106,6 +107,7 @@ struct qg_hamiltonian_s {
     DevProjectors pj;
     DevBuf coef;      // projector coefficients E*dV*<p|psi>, [ns][na*nch]
     DevBuf xio, hxio; // staging for the host-buffer entry point
+    DevBuf kco;       // per-k-point stencil coefficients of a multi-k apply
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
     qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
@@ -158,5 +160,11 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
 // imaginary part N elements later; coef_scratch holds 2*coef_scratch_elems(h, ns) doubles.
 int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
                         double* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
+// Several k-points in one pass: nk k-vectors kv (3 each, bohr^-1), nsk states per k-point,
+// state s of k-point k at X + k*ldk + s*ldx (HX + k*ldkh + s*ldhx); coef_scratch holds
+// 2*coef_scratch_elems(h, nk*nsk) doubles.
+int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, const double* X, long long ldx,
+                         long long ldk, double* HX, long long ldhx, long long ldkh, double* coef_scratch,
+                         cudaStream_t st, PhaseTimer* pt = nullptr);
 
 }  // namespace qg

@@ -31,7 +31,21 @@ struct HamArgs {
     // axis whose |g| < 1e-8), c0 then carries the -coef*|g|^2 term
     long long xim, hxim;
     T dx[4], dy[4], dz[4];
+    // several k-points in one launch (NC = 2): states are grouped by k, nsk per k;
+    // state s of k-point k starts at X + k*ldkx + s*ldx (HX + k*ldkhx + s*ldhx), and
+    // kco[k*13 + {0, 1..4, 5..8, 9..12}] replaces c0, dx, dy, dz (nsk = 0: one k-point)
+    int nsk;
+    long long ldkx, ldkhx;
+    const T* kco;
 };
+
+// first element of global state index s (k-point major when several k-points share a launch)
+template <typename T>
+__device__ __forceinline__ long long state_offset(const HamArgs<T>& a, int s, bool out) {
+    if (a.nsk <= 0) return (long long)s * (out ? a.ldhx : a.ldx);
+    const int k = s / a.nsk, sl = s - k * a.nsk;
+    return out ? (long long)k * a.ldkhx + (long long)sl * a.ldhx : (long long)k * a.ldkx + (long long)sl * a.ldx;
+}
 
 __device__ __forceinline__ int wrap_idx(int i, int n) {
     i %= n;

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
                 const int y0 = tile * ty;
                 const int zs = slab * wg.zslab;
                 const int ze = min(nz, zs + wg.zslab);
-                const T* Xs = a.X + (long long)s * a.ldx;
+                const T* Xs = a.X + state_offset(a, s, false);
                 for (int p = zs - R; p <= ze - 1 + R; ++p, ++pos) {
                     const int j = pos % nst;
                     const int k = pos / nst;
@@ -292,7 +292,19 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
             if (lane != 0) jz = (pos + R) % nst;
             int jp = j;             // stage of plane z + R (= position pos + 2R)
             uint32_t php = ph;
-            T* hxp = a.HX + (long long)s * a.ldhx + (long long)zs * plane + col;
+            T* hxp = a.HX + state_offset(a, s, true) + (long long)zs * plane + col;
+            // per-k-point coefficients of the k-point kinetic term
+            HamArgs<T> ak = a;
+            if (NC == 2 && a.kco) {
+                const T* kc = a.kco + (long long)(s / a.nsk) * 13;
+                ak.c0 = kc[0];
+#pragma unroll
+                for (int d = 0; d < 4; ++d) {
+                    ak.dx[d] = kc[1 + d];
+                    ak.dy[d] = kc[5 + d];
+                    ak.dz[d] = kc[9 + d];
+                }
+            }
             for (int z = zs; z < ze; ++z) {
                 if (z + R < ze) vq[R].v = *reinterpret_cast<const VT*>(vp);
                 vp += plane;
@@ -336,8 +348,8 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
                             zm[d - 1] = q[cc][R - d].e[e];
                             zp[d - 1] = q[cc][R + d].e[e];
                         }
-                        lap[cc][e] = lap_point<T, ORDER>(q[cc][R].e[e], xm, xp, ym, yp, zm, zp, a);
-                        if constexpr (NC == 2) der[cc][e] = der_point<T>(xm, xp, ym, yp, zm, zp, a);
+                        lap[cc][e] = lap_point<T, ORDER>(q[cc][R].e[e], xm, xp, ym, yp, zm, zp, ak);
+                        if constexpr (NC == 2) der[cc][e] = der_point<T>(xm, xp, ym, yp, zm, zp, ak);
                     }
                 }
                 __syncwarp(wmask);

@@ -120,3 +120,28 @@ def test_kpoint_invalid_arguments(cuda_ctx):
     assert lib().qg_hamiltonian_apply_z(H6.h, 2, C.c_void_p(X.data_ptr()), 2 * cell.N, C.c_void_p(Y.data_ptr()),
                                         2 * cell.N) == -7
     H6.close()
+
+
+@pytest.mark.parametrize("plain", [False, True], ids=["tma", "plain"])
+def test_multi_kpoint_apply_in_one_pass(cuda_ctx, plain):
+    """qg_hamiltonian_apply_zk over 5 Monkhorst-Pack k-points x 3 states equals the
+    single-k operator applied k-point by k-point, and the oracle."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(grid=(24, 20, 16), displacement=0.05, seed=3)
+    N = cell.N
+    b = 2 * np.pi / (cell.nx * cell.hx)
+    kv = np.array([[0.125, 0.375, -0.125], [0.0, 0.0, 0.0], [-0.375, 0.125, 0.375], [0.25, 0.25, 0.25],
+                   [0.5, -0.5, 0.0]]) * b
+    X = initial_states(15, 2 * N, seed=41).reshape(5, 3, 2 * N)
+    H = Hamiltonian(cuda_ctx, cell)
+    H.set_stencil_kernel(plain)
+    Xd = torch.from_numpy(X).cuda()
+    many = H.apply_zk(kv, Xd).cpu().numpy()
+    for k in range(5):
+        H.set_kvector(kv[k])
+        one = H.apply_z(Xd[k]).cpu().numpy()
+        np.testing.assert_array_equal(many[k], one)
+        ref = O.hamiltonian_kpoint_apply(cell, tuple(kv[k]), X[k])
+        assert rel_per_state(many[k], ref).max() < TOL64
+    H.close()
