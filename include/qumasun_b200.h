@@ -249,6 +249,17 @@ int qg_lobpcg_d_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns,
  * as called by qumasun_kpoint.lobpcg.h:32-41. */
 int qg_lobpcg_z(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
                 double* P, qg_lobpcg_report* report);
+/* Complex LOBPCG for nk k-points in one solve (the batched form of running
+ * qg_lobpcg_z once per k-point): kvecs = nk Bloch vectors (HOST, 3 each), nsk states
+ * per k-point, X and P DEVICE, [k][s] state-major ({re[N], im[N]} per state), ev HOST
+ * (nk * nsk). H, norms, residuals and the preconditioner run over all k-points' states in
+ * single launches; Gram products and rotations are strided-batched DGEMMs over k; the
+ * nsk-state pencils are solved k-point by k-point. FP64; precond 0 or 1; stops when the
+ * lowest n_converge states of every k-point meet tol. The report carries iterations,
+ * convergence, max_residual, ms_total and restarts. No counterpart in the reference,
+ * which loops over k-points (qumasun_kpoint.lobpcg.h:25-41). */
+int qg_lobpcg_zk_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int nk, const double* kvecs, int nsk,
+                        double* ev, double* X, double* P, qg_lobpcg_report* report);
 /* Same with DEVICE buffers X and P (ld = 2N); ev stays a host array. */
 int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
                        double* X, double* P, qg_lobpcg_report* report);

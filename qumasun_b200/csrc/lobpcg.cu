@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "gram_mixed.h"
@@ -772,6 +773,230 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     return converged ? QG_OK : QG_ERR_NOT_CONVERGED;
 }
 
+// Complex block LOBPCG for nk k-points at once (block-diagonal Rayleigh-Ritz).
+// All nk*nb states live in the same W / AW / T blocks, k-point major ([k][s], each
+// state {re[N], im[N]}), so H, norms, residuals and the preconditioner run over all
+// of them in single launches (qg::apply_hamiltonian_zk for H). The Gram products
+// and rotations of the k-points are strided-batched DGEMMs (one per block pair of
+// [x r p], batched over k); the small Hermitian pencils are solved k by k
+// (Jacobi-equilibrated cusolverDnZhegvd, the rank-revealing solve where B is
+// singular). Stops when every k-point's lowest n_converge states meet tol.
+int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const double* kv, int nb, double* ev,
+                  double* X_dev, double* P_dev, qg_lobpcg_report* rep) {
+    if (!h || !opt || nk <= 0 || nb <= 0 || !kv || !ev || !X_dev) return QG_ERR_INVALID;
+    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
+    if (opt->precond < 0 || opt->precond > 1) return QG_ERR_INVALID;
+    const long long N = h->N();
+    if ((long long)nb * 3 > N) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    const int nt = nk * nb;
+    Solver s;
+    s.h = h;
+    s.n = nt;
+    s.c = 2;
+    s.N = N;
+    s.L = 2 * N;
+    s.dV = h->hx * h->hy * h->hz;
+    s.st = h->ctx->stream;
+    cudaStream_t st = s.st;
+    QG_TRY(qg_blas_handle(h->ctx, &s.blas));
+    QG_TRY(qg_solver_handle(h->ctx, &s.sol));
+    // tall blocks for all states, Gram pencils and rotations per k-point
+    const size_t blk = (size_t)s.L * nt;
+    QG_TRY(s.W.reserve(3 * blk * sizeof(double)));
+    QG_TRY(s.AW.reserve(3 * blk * sizeof(double)));
+    QG_TRY(s.T.reserve(2 * blk * sizeof(double)));
+    s.x = s.W.as<double>(); s.r = s.x + blk; s.p = s.r + blk;
+    s.Ax = s.AW.as<double>(); s.Ar = s.Ax + blk; s.Ap = s.Ar + blk;
+    s.Tx = s.T.as<double>(); s.Tp = s.Tx + blk;
+    const int k3m = 3 * nb, g3 = 2 * k3m;
+    const size_t gsz = (size_t)g3 * g3, msz = (size_t)g3 * 2 * nb, kk = (size_t)k3m * k3m;
+    QG_TRY(s.S.reserve((2 * nk * gsz + 4 * kk + nk * msz) * sizeof(double)));
+    QG_CUDA_TRY(cudaMemsetAsync(s.S.ptr, 0, s.S.bytes, st));
+    double* SaAll = s.S.as<double>();
+    double* SbAll = SaAll + nk * gsz;
+    s.Sa2 = SbAll + nk * gsz;
+    s.Sb2 = s.Sa2 + 2 * kk;
+    double* Mall = s.Sb2 + 2 * kk;
+    s.Ca = reinterpret_cast<cuDoubleComplex*>(s.Sa2);
+    s.Cb = reinterpret_cast<cuDoubleComplex*>(s.Sb2);
+    QG_TRY(s.E.reserve(8 * kk * sizeof(double)));
+    s.E0 = s.E.as<double>();
+    s.s_h.resize(k3m);
+    QG_TRY(s.small.reserve(((size_t)5 * 3 * nt + 16 + nk) * sizeof(double)));
+    s.ev_d = s.small.as<double>(); s.nr_d = s.ev_d + 3 * nt; s.f_d = s.nr_d + 3 * nt; s.f2_d = s.f_d + 3 * nt;
+    s.w_d = s.f2_d + 3 * nt;
+    s.info_d = reinterpret_cast<int*>(s.w_d + 3 * nt);
+    int* infos_d = s.info_d + 4;
+    {
+        int lw1 = 0, lw2 = 0;
+        QG_SOLVER_TRY(cusolverDnZhegvd_bufferSize(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                  CUBLAS_FILL_MODE_LOWER, k3m, s.Ca, k3m, s.Cb, k3m, s.w_d, &lw1));
+        QG_SOLVER_TRY(cusolverDnZheevd_bufferSize(s.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k3m, s.Cb,
+                                                  k3m, s.w_d, &lw2));
+        s.lwork = std::max(lw1, lw2);
+        QG_TRY(s.work.reserve((size_t)std::max(s.lwork, 1) * sizeof(cuDoubleComplex)));
+    }
+    QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, nt) * sizeof(double)));
+    const size_t blk_bytes = blk * sizeof(double);
+    const bool first = opt->first_call != 0;
+    const double tol = opt->tol > 0 ? opt->tol : 1.0e-10;
+    const int nconv = (opt->n_converge > 0 && opt->n_converge < nb) ? opt->n_converge : nb;
+    const long long kstride = 2LL * nb * N;  // one k-point's columns within a block
+    auto applyH = [&](const double* in, double* out) {
+        return qg::apply_hamiltonian_zk(h, nk, kv, nb, in, s.L, (long long)nb * s.L, out, s.L, (long long)nb * s.L,
+                                        h->coef.as<double>(), st);
+    };
+    // C_k (block (bi, bj) of the k-th pencil, ldc g) = dV * A_k^T B_k, batched over k
+    auto gram_block = [&](const double* A, const double* B, double* C, int g) -> int {
+        const double zero = 0.0;
+        QG_BLAS_TRY(cublasDgemmStridedBatched(s.blas, CUBLAS_OP_T, CUBLAS_OP_N, 2 * nb, 2 * nb, (int)N, &s.dV, A,
+                                              (int)N, kstride, B, (int)N, kstride, &zero, C, g, (long long)gsz, nk));
+        return QG_OK;
+    };
+    // C_k (N x 2nb) = A_k (N x 2nb) * Z_k (rows off.., ldz) + beta C_k, batched over k
+    auto rot_block = [&](const double* A, const double* Z, int ldz, double* C, double beta) -> int {
+        const double one = 1.0;
+        QG_BLAS_TRY(cublasDgemmStridedBatched(s.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, 2 * nb, 2 * nb, &one, A,
+                                              (int)N, kstride, Z, ldz, (long long)msz, &beta, C, (int)N, kstride, nk));
+        return QG_OK;
+    };
+    cudaEvent_t t0, t1;
+    QG_CUDA_TRY(cudaEventCreate(&t0));
+    QG_CUDA_TRY(cudaEventCreate(&t1));
+    QG_CUDA_TRY(cudaEventRecord(t0, st));
+    QG_CUDA_TRY(cudaMemcpyAsync(s.x, X_dev, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    if (first || !P_dev) QG_CUDA_TRY(cudaMemsetAsync(s.p, 0, blk_bytes, st));
+    else QG_CUDA_TRY(cudaMemcpyAsync(s.p, P_dev, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    s.normalize(s.x, nullptr);
+    QG_TRY(applyH(s.x, s.Ax));
+    if (first || !P_dev) QG_CUDA_TRY(cudaMemsetAsync(s.Ap, 0, blk_bytes, st));
+    else QG_TRY(applyH(s.p, s.Ap));
+    s.coldot(s.x, s.Ax, s.dV, s.ev_d);
+    s.residual();
+    qg::KineticPrecond* pc = nullptr;
+    if (opt->precond == 1) {
+        if (!h->precond) h->precond = new qg::KineticPrecond();
+        pc = h->precond;
+        QG_TRY(pc->setup(h, 2 * nt, opt->precond_shift > 0 ? opt->precond_shift : 1.0));
+        QG_TRY(pc->apply(s.r, st));
+        s.normalize(s.r, nullptr);
+    } else {
+        k_inv_norm<<<(nt + 127) / 128, 128, 0, st>>>(s.nr_d, 1.0, nt, s.f_d);
+        s.scale_cols(s.r, nullptr);
+    }
+    QG_CUDA_TRY(cudaGetLastError());
+    std::vector<double> ev_h(nt), nr_h(nt);
+    std::vector<int> info_h(nk);
+    int it = 0, restarts = 0, status = QG_OK;
+    bool converged = false;
+    double maxres = 0.0;
+    for (it = 0; it < opt->max_iter; ++it) {
+        QG_TRY(applyH(s.r, s.Ar));
+        const bool two = first && it == 0;
+        const int k3 = (two ? 2 : 3) * nb, g = 2 * k3;
+        const double* Wb[3] = {s.x, s.r, s.p};
+        const double* AWb[3] = {s.Ax, s.Ar, s.Ap};
+        for (int bi = 0; bi < k3 / nb; ++bi)
+            for (int bj = 0; bj <= bi; ++bj) {
+                const size_t off = (size_t)bi * 2 * nb + (size_t)bj * 2 * nb * g;
+                QG_TRY(gram_block(Wb[bi], AWb[bj], SaAll + off, g));
+                QG_TRY(gram_block(Wb[bi], Wb[bj], SbAll + off, g));
+            }
+        // Hermitian pencils k by k; solutions expanded to real rotations M_k (2k3 x 2nb)
+        for (int k = 0; k < nk; ++k) {
+            double* Sa_k = SaAll + k * gsz;
+            double* Sb_k = SbAll + k * gsz;
+            k_gram_to_complex<<<k3, 128, 0, st>>>(Sa_k, Sb_k, g, k3, s.Ca, s.Cb, k3);
+            QG_SOLVER_TRY(cusolverDnZhegvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           k3, s.Ca, k3, s.Cb, k3, s.w_d, s.work.as<cuDoubleComplex>(), s.lwork,
+                                           infos_d + k));
+            k_expand_rotation<<<nb, 128, 0, st>>>(s.Ca, k3, k3, k3, Sb_k, g, Mall + k * msz, g);
+        }
+        QG_CUDA_TRY(cudaMemcpyAsync(info_h.data(), infos_d, nk * sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int k = 0; k < nk && status == QG_OK; ++k) {
+            if (info_h[k] == 0) continue;
+            if (info_h[k] < 0) {
+                status = QG_ERR_LIBRARY;
+                break;
+            }
+            ++restarts;
+            s.Sa = SaAll + k * gsz;
+            s.Sb = SbAll + k * gsz;
+            s.M = Mall + k * msz;
+            const double* Z = nullptr;
+            int ldz = 0;
+            s.n = nb;  // the pencil's eigenvectors kept: one k-point's states
+            const int rc = s.solve_truncated(k3, k3, &Z, &ldz);
+            s.n = nt;
+            if (rc == QG_ERR_CHOLESKY) status = QG_ERR_CHOLESKY;
+            else if (rc != QG_OK) return rc;
+        }
+        if (status != QG_OK) {
+            ++it;
+            break;
+        }
+        // rotation, batched over k: p_new = r Cr (+ p Cp), x_new = x Cx + p_new
+        QG_TRY(rot_block(s.r, Mall + 2 * nb, g, s.Tp, 0.0));
+        if (!two) QG_TRY(rot_block(s.p, Mall + 4 * nb, g, s.Tp, 1.0));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_TRY(rot_block(s.x, Mall, g, s.Tx, 1.0));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        s.normalize(s.x, nullptr);
+        s.normalize(s.p, nullptr);
+        QG_TRY(applyH(s.x, s.Ax));
+        QG_TRY(applyH(s.p, s.Ap));
+        s.coldot(s.x, s.Ax, s.dV, s.ev_d);
+        s.residual();
+        QG_CUDA_TRY(cudaGetLastError());
+        QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (pc) {
+            QG_TRY(pc->apply(s.r, st));
+            s.normalize(s.r, nullptr);
+        }
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        maxres = 0.0;
+        for (int j = 0; j < nt; ++j)
+            if (j % nb < nconv) maxres = std::max(maxres, nr_h[j]);
+        if (!std::isfinite(maxres)) {
+            status = QG_ERR_NONFINITE;
+            ++it;
+            break;
+        }
+        if (opt->verbose) printf("lobpcg(%d k-points) iter %d max residual %.3e\n", nk, it + 1, maxres);
+        if (maxres < tol * s.dV) {
+            converged = true;
+            ++it;
+            break;
+        }
+    }
+    QG_CUDA_TRY(cudaMemcpyAsync(ev_h.data(), s.ev_d, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QG_CUDA_TRY(cudaMemcpyAsync(X_dev, s.x, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    if (P_dev) QG_CUDA_TRY(cudaMemcpyAsync(P_dev, s.p, blk_bytes, cudaMemcpyDeviceToDevice, st));
+    QG_CUDA_TRY(cudaEventRecord(t1, st));
+    QG_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int j = 0; j < nt; ++j) ev[j] = ev_h[j];
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rep) {
+        std::memset(rep, 0, sizeof(*rep));
+        rep->iterations = it;
+        rep->converged = converged ? 1 : 0;
+        rep->max_residual = maxres;
+        rep->ms_total = tot;
+        rep->restarts = restarts;
+    }
+    const int dstat = qg_context_take_device_status(h->ctx);
+    if (dstat != QG_OK) return dstat;
+    if (status != QG_OK) return status;
+    return converged ? QG_OK : QG_ERR_NOT_CONVERGED;
+}
+
 }  // namespace
 
 extern "C" {
@@ -792,6 +1017,12 @@ int qg_lobpcg_z(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* 
                 qg_lobpcg_report* rep) {
     if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
     return run_lobpcg(h, opt, ns, 2, ev, nullptr, nullptr, X, X, P, P, rep);
+}
+
+int qg_lobpcg_zk_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const double* kvecs, int nsk,
+                        double* ev, double* X, double* P, qg_lobpcg_report* rep) {
+    if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
+    return run_lobpcg_zk(h, opt, nk, kvecs, nsk, ev, X, P, rep);
 }
 
 int qg_lobpcg_z_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,

@@ -134,6 +134,8 @@ def lib():
         L.qg_hamiltonian_set_learned.argtypes = [vp, vp, C.c_double]
         L.qg_hamiltonian_precondition_d.argtypes = [vp, C.c_int, vp, C.c_longlong, C.c_double]
         L.qg_lobpcg_z.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
+        L.qg_lobpcg_zk_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, C.c_int, _dp, vp, vp,
+                                          C.POINTER(LobpcgReport)]
         L.qg_lobpcg_z_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
         L.qg_lobpcg_d_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
@@ -373,6 +375,25 @@ class Hamiltonian:
         if st not in (QG_OK, -9):
             check(st, "qg_lobpcg_z_device" if complex_states else "qg_lobpcg_d_device")
         return dict(ev=ev, report=rep.as_dict(), status=st)
+
+    def lobpcg_zk(self, kvecs, X, P=None, max_iter=2000, tol=1.0e-10, first=True, verbose=False, precond=0,
+                  shift=1.0, n_converge=0):
+        """Complex LOBPCG for several k-points in one solve: X float64 CUDA tensor
+        (nk, nsk, 2N) overwritten with the eigenvectors; returns dict(ev (nk, nsk), report, status)."""
+        import torch
+        assert X.is_cuda and X.dim() == 3 and X.is_contiguous() and X.dtype == torch.float64
+        kv = np.ascontiguousarray(np.asarray(kvecs, dtype=np.float64).reshape(-1, 3))
+        nk, nsk = X.shape[0], X.shape[1]
+        ev = np.zeros(nk * nsk)
+        opt = LobpcgOptions(max_iter, tol, 1 if first else 0, 0, 1 if verbose else 0, precond, shift, n_converge)
+        rep = LobpcgReport()
+        self.ctx.use_torch_stream()
+        st = lib().qg_lobpcg_zk_device(self.h, C.byref(opt), nk, kv.ctypes.data_as(_dp), nsk,
+                                       ev.ctypes.data_as(_dp), C.c_void_p(X.data_ptr()),
+                                       C.c_void_p(P.data_ptr() if P is not None else 0), C.byref(rep))
+        if st not in (QG_OK, -9):
+            check(st, "qg_lobpcg_zk_device")
+        return dict(ev=ev.reshape(nk, nsk), report=rep.as_dict(), status=st)
 
     def lobpcg_z(self, X0, max_iter=2000, tol=1.0e-10, P0=None, first=True, verbose=False, precond=0,
                  shift=1.0):

@@ -83,3 +83,27 @@ def test_diamond8_kpoint_mixed_precision(cuda_ctx, gold):
     H.close()
     assert r["status"] == 0 and r["report"]["converged"] == 1
     np.testing.assert_allclose(np.sort(r["ev"]), gold["d8_lanczos"][:16], rtol=0, atol=TOL_EV)
+
+
+def test_batched_kpoints_match_one_by_one_solves(cuda_ctx, gold):
+    """qg_lobpcg_zk_device over 4 Monkhorst-Pack k-points (the golden one among them)
+    gives every k-point the eigenvalues of its own single-k solve (and the golden
+    k-point the Lanczos values) to 1e-8 Ha."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell()
+    b = 2 * np.pi / 6.74
+    kv = np.array([gold["d8_g"], np.array([0.375, 0.125, 0.125]) * b, np.array([-0.125, -0.125, 0.375]) * b,
+                   np.zeros(3)])
+    ns = 16
+    X0 = initial_states(ns, 2 * cell.N, seed=int(gold["d8_seed"]))
+    H = Hamiltonian(cuda_ctx, cell)
+    X = torch.from_numpy(np.stack([X0] * 4)).cuda().contiguous()
+    r = H.lobpcg_zk(kv, X, max_iter=500, precond=1, tol=1e-12, n_converge=14)
+    assert r["status"] == 0 and r["report"]["converged"] == 1
+    np.testing.assert_allclose(np.sort(r["ev"][0])[:14], gold["d8_lanczos"][:14], rtol=0, atol=TOL_EV)
+    for k in range(4):
+        H.set_kvector(kv[k])
+        one = H.lobpcg_z(X0, max_iter=500, precond=1, tol=1e-12)
+        np.testing.assert_allclose(np.sort(r["ev"][k])[:14], np.sort(one["ev"])[:14], rtol=0, atol=TOL_EV)
+    H.close()
