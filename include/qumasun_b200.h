@@ -253,8 +253,9 @@ int qg_lobpcg_z(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double
  * qg_lobpcg_z once per k-point): kvecs = nk Bloch vectors (HOST, 3 each), nsk states
  * per k-point, X and P DEVICE, [k][s] state-major ({re[N], im[N]} per state), ev HOST
  * (nk * nsk). H, norms, residuals and the preconditioner run over all k-points' states in
- * single launches; Gram products and rotations are strided-batched DGEMMs over k; the
- * nsk-state pencils are solved k-point by k-point. FP64; precond 0 or 1; stops when the
+ * single launches; Gram products are DGEMMs per k-point, rotations strided-batched DGEMMs
+ * over k; the nsk-state pencils are solved k-point by k-point, and a k-point whose states
+ * have converged is frozen (no further rotation or solve). FP64; precond 0 or 1; stops when the
  * lowest n_converge states of every k-point meet tol. The report carries iterations,
  * convergence, max_residual, ms_total and restarts. No counterpart in the reference,
  * which loops over k-points (qumasun_kpoint.lobpcg.h:25-41). */

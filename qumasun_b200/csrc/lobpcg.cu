@@ -125,7 +125,7 @@ __global__ void k_scale_cols(double* __restrict__ A, double* __restrict__ B, lon
 // f[j] = 1 / sqrt(norm2[j] * dV)   (Normalize, vecmath.h:128-133)
 __global__ void k_inv_norm(const double* __restrict__ norm2, double dV, int n, double* __restrict__ f) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) f[j] = 1.0 / sqrt(norm2[j] * dV);
+    if (j < n) f[j] = norm2[j] > 0.0 ? 1.0 / sqrt(norm2[j] * dV) : 0.0;  // a zero column stays zero
 }
 
 // r_j = Ax_j - ei_j x_j and nr[j] = dV * sum_i r_j(i)^2   (lobpcg_d_multi.h:506-516)
@@ -239,6 +239,13 @@ __global__ void k_scaled_basis(const T* __restrict__ V, int ld, int k, const dou
         if constexpr (sizeof(T) == 16) Tm[i + (long long)j * ld] = make_cuDoubleComplex(cuCreal(v) * sc, cuCimag(v) * sc);
         else Tm[i + (long long)j * ld] = v * sc;
     }
+}
+
+// Rotation of a k-point whose states have converged: x_new = x, p_new = 0
+// (M = [I; 0; 0], 2k3 x 2nb, ld g); one block per column.
+__global__ void k_freeze_rotation(double* __restrict__ M, int g, int rows) {
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) M[i + (long long)j * g] = (i == j) ? 1.0 : 0.0;
 }
 
 struct Timer {
@@ -777,8 +784,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
 // All nk*nb states live in the same W / AW / T blocks, k-point major ([k][s], each
 // state {re[N], im[N]}), so H, norms, residuals and the preconditioner run over all
 // of them in single launches (qg::apply_hamiltonian_zk for H). The Gram products
-// and rotations of the k-points are strided-batched DGEMMs (one per block pair of
-// [x r p], batched over k); the small Hermitian pencils are solved k by k
+// are DGEMMs per k-point and block pair of [x r p], the rotations strided-batched
+// DGEMMs over k; the small Hermitian pencils are solved k by k
 // (Jacobi-equilibrated cusolverDnZhegvd, the rank-revealing solve where B is
 // singular). Stops when every k-point's lowest n_converge states meet tol.
 int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const double* kv, int nb, double* ev,
@@ -848,11 +855,15 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         return qg::apply_hamiltonian_zk(h, nk, kv, nb, in, s.L, (long long)nb * s.L, out, s.L, (long long)nb * s.L,
                                         h->coef.as<double>(), st);
     };
-    // C_k (block (bi, bj) of the k-th pencil, ldc g) = dV * A_k^T B_k, batched over k
+    // C_k (block (bi, bj) of the k-th pencil, ldc g) = dV * A_k^T B_k, one DGEMM per k-point:
+    // cuBLAS's strided-batched DGEMM at these shapes (2nb x 2nb, K = N) returned Gram
+    // matrices noticeably less accurate than its plain DGEMM (8 k-points: 208 rank-revealing
+    // restarts and 95 iterations instead of 11 and 73), so the batch is a loop of DGEMMs
     auto gram_block = [&](const double* A, const double* B, double* C, int g) -> int {
         const double zero = 0.0;
-        QG_BLAS_TRY(cublasDgemmStridedBatched(s.blas, CUBLAS_OP_T, CUBLAS_OP_N, 2 * nb, 2 * nb, (int)N, &s.dV, A,
-                                              (int)N, kstride, B, (int)N, kstride, &zero, C, g, (long long)gsz, nk));
+        for (int k = 0; k < nk; ++k)
+            QG_BLAS_TRY(cublasDgemm(s.blas, CUBLAS_OP_T, CUBLAS_OP_N, 2 * nb, 2 * nb, (int)N, &s.dV, A + k * kstride,
+                                    (int)N, B + k * kstride, (int)N, &zero, C + k * gsz, g));
         return QG_OK;
     };
     // C_k (N x 2nb) = A_k (N x 2nb) * Z_k (rows off.., ldz) + beta C_k, batched over k
@@ -889,6 +900,10 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
     QG_CUDA_TRY(cudaGetLastError());
     std::vector<double> ev_h(nt), nr_h(nt);
     std::vector<int> info_h(nk);
+    // a k-point whose lowest n_converge states meet tol is frozen: its states are no
+    // longer rotated and its pencil is no longer solved, so the solve ends after as
+    // many iterations as the slowest k-point needs on its own
+    std::vector<char> frozen(nk, 0);
     int it = 0, restarts = 0, status = QG_OK;
     bool converged = false;
     double maxres = 0.0;
@@ -905,9 +920,14 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
                 QG_TRY(gram_block(Wb[bi], Wb[bj], SbAll + off, g));
             }
         // Hermitian pencils k by k; solutions expanded to real rotations M_k (2k3 x 2nb)
+        QG_CUDA_TRY(cudaMemsetAsync(infos_d, 0, nk * sizeof(int), st));
         for (int k = 0; k < nk; ++k) {
             double* Sa_k = SaAll + k * gsz;
             double* Sb_k = SbAll + k * gsz;
+            if (frozen[k]) {
+                k_freeze_rotation<<<2 * nb, 128, 0, st>>>(Mall + k * msz, g, g);
+                continue;
+            }
             k_gram_to_complex<<<k3, 128, 0, st>>>(Sa_k, Sb_k, g, k3, s.Ca, s.Cb, k3);
             QG_SOLVER_TRY(cusolverDnZhegvd(s.sol, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
                                            k3, s.Ca, k3, s.Cb, k3, s.w_d, s.work.as<cuDoubleComplex>(), s.lwork,
@@ -959,15 +979,21 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         }
         QG_CUDA_TRY(cudaStreamSynchronize(st));
         maxres = 0.0;
-        for (int j = 0; j < nt; ++j)
-            if (j % nb < nconv) maxres = std::max(maxres, nr_h[j]);
+        bool all = true;
+        for (int k = 0; k < nk; ++k) {
+            double mk = 0.0;
+            for (int j = 0; j < nconv; ++j) mk = std::max(mk, nr_h[k * nb + j]);
+            if (mk < tol * s.dV) frozen[k] = 1;
+            if (!frozen[k]) all = false;
+            if (!frozen[k] || mk < tol * s.dV) maxres = std::max(maxres, mk);
+        }
         if (!std::isfinite(maxres)) {
             status = QG_ERR_NONFINITE;
             ++it;
             break;
         }
         if (opt->verbose) printf("lobpcg(%d k-points) iter %d max residual %.3e\n", nk, it + 1, maxres);
-        if (maxres < tol * s.dV) {
+        if (all) {
             converged = true;
             ++it;
             break;
