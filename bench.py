@@ -376,6 +376,8 @@ def kpoint_leg(ctx, n_k=64, steps=10, rank=0, ws=1):
             diff = float(max(np.abs(np.sort(evb[i]) - np.sort(np.array(res[i]["ev"]))).max() for i in range(n_k)))
         batched = {"mode": "all k-points in one solve (qg_lobpcg_zk_device)", "k_points": n_k, "seconds": round(wb, 3),
                    "device_ms": round(rb["report"]["ms_total"], 1), "iterations": rb["report"]["iterations"],
+                   "phase_ms": {k_: round(rb["report"][k_], 1) for k_ in ("ms_hamiltonian", "ms_gram", "ms_eigensolve",
+                                                                         "ms_rotate", "ms_vector")},
                    "converged": bool(rb["report"]["converged"]), "max_abs_ev_diff_vs_one_by_one_Ha": diff}
         del Xb
     H.close()

@@ -907,8 +907,11 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
     int it = 0, restarts = 0, status = QG_OK;
     bool converged = false;
     double maxres = 0.0;
+    Timer tm;
     for (it = 0; it < opt->max_iter; ++it) {
+        tm.mark(0, st);
         QG_TRY(applyH(s.r, s.Ar));
+        tm.mark(1, st);
         const bool two = first && it == 0;
         const int k3 = (two ? 2 : 3) * nb, g = 2 * k3;
         const double* Wb[3] = {s.x, s.r, s.p};
@@ -920,6 +923,7 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
                 QG_TRY(gram_block(Wb[bi], Wb[bj], SbAll + off, g));
             }
         // Hermitian pencils k by k; solutions expanded to real rotations M_k (2k3 x 2nb)
+        tm.mark(2, st);
         QG_CUDA_TRY(cudaMemsetAsync(infos_d, 0, nk * sizeof(int), st));
         for (int k = 0; k < nk; ++k) {
             double* Sa_k = SaAll + k * gsz;
@@ -958,6 +962,7 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
             ++it;
             break;
         }
+        tm.mark(3, st);
         // rotation, batched over k: p_new = r Cr (+ p Cp), x_new = x Cx + p_new
         QG_TRY(rot_block(s.r, Mall + 2 * nb, g, s.Tp, 0.0));
         if (!two) QG_TRY(rot_block(s.p, Mall + 4 * nb, g, s.Tp, 1.0));
@@ -965,10 +970,13 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         QG_TRY(rot_block(s.x, Mall, g, s.Tx, 1.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        tm.mark(4, st);
         s.normalize(s.x, nullptr);
         s.normalize(s.p, nullptr);
+        tm.mark(0, st);
         QG_TRY(applyH(s.x, s.Ax));
         QG_TRY(applyH(s.p, s.Ap));
+        tm.mark(4, st);
         s.coldot(s.x, s.Ax, s.dV, s.ev_d);
         s.residual();
         QG_CUDA_TRY(cudaGetLastError());
@@ -977,7 +985,9 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
             QG_TRY(pc->apply(s.r, st));
             s.normalize(s.r, nullptr);
         }
+        tm.mark(-1, st);
         QG_CUDA_TRY(cudaStreamSynchronize(st));
+        tm.flush();
         maxres = 0.0;
         bool all = true;
         for (int k = 0; k < nk; ++k) {
@@ -1015,6 +1025,11 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         rep->converged = converged ? 1 : 0;
         rep->max_residual = maxres;
         rep->ms_total = tot;
+        rep->ms_hamiltonian = tm.acc[0];
+        rep->ms_gram = tm.acc[1];
+        rep->ms_eigensolve = tm.acc[2];
+        rep->ms_rotate = tm.acc[3];
+        rep->ms_vector = tm.acc[4];
         rep->restarts = restarts;
     }
     const int dstat = qg_context_take_device_status(h->ctx);
