@@ -25,7 +25,8 @@ def needs_build():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    deps = (sources() + glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))
+            + glob.glob(os.path.join(ROOT, "include", "*.h")))
     return any(os.path.getmtime(f) > t for f in deps)
 
 

@@ -2,11 +2,11 @@
 //   H psi = V psi + sum_atoms sum_k E_k sum_m |p_km> dV <p_km|psi> - 1/2 Lap psi.
 //
 // Main path (shapes the TMA kernel accepts), three launches for a block of states:
-//   k_project     c[s][a,ch] = E_ch dV sum_{p in sphere(a)} tab[ch][p] psi_s[g(p)]
+//   k_project     c[a,ch][s] = E_ch dV sum_{p in sphere(a)} tab[ch][p] psi_s[g(p)]
 //                 (InnerProd_1S_1R / InnerProd_2S_1R of ProjectionPP, PseudoPotOperator.h:740-772,
 //                 all atoms, channels and states at once);
 //   k_stencil_tma H psi = V psi - 1/2 Lap psi (stencil_tma.cu: persistent, TMA-staged);
-//   k_scatter_all H psi[s][g] += sum_{entries e of g} sum_ch val[e][ch] c[s][a_e,ch]
+//   k_scatter_all H psi[s][g] += sum_{entries e of g} sum_ch val[e][ch] c[a_e,ch][s]
 //                 (Add_1S / Add_2S of ProjectionPP turned into a per-point gather, no atomics).
 // Fallback path (any shape): k_project, then k_hamiltonian, a register-window
 // stencil kernel with the per-point scatter fused in.
@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "qg_internal.h"
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(1024) k_hamiltonian(const HamArgs<T> a) {
                     const T tv = ev[ch];
 #pragma unroll
                     for (int s = 0; s < SPB; ++s)
-                        nl[s] += tv * a.coef[(long long)(valid[s] ? s0 + s : s0) * a.ncoef + at * a.nch + ch];
+                        nl[s] += tv * a.coef[(long long)(at * a.nch + ch) * a.ldc + (valid[s] ? s0 + s : s0)];
                 }
             }
         }
@@ -191,13 +192,15 @@ __global__ void __launch_bounds__(1024) k_hamiltonian(const HamArgs<T> a) {
 }
 
 // Gather-contraction of the projectors: one block per (atom, group of SB states).
+// The coefficients are stored channel-major, coef[(atom * NCH + ch) * ldc + s], so
+// that the scatter reads the states of one (atom, channel) as contiguous vectors.
 template <typename T, int SB, int NCH>
 __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long long ldx, int ns,
                                                  const int* __restrict__ atom_off,
                                                  const int* __restrict__ pt_g,
                                                  const T* __restrict__ tab, long long npts,
                                                  const double* __restrict__ ch_scale,
-                                                 T* __restrict__ coef, int ncoef) {
+                                                 T* __restrict__ coef, long long ldc) {
     const int atom = blockIdx.x;
     const int s0 = blockIdx.y * SB;
     const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
@@ -206,22 +209,44 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
     for (int s = 0; s < SB; ++s)
 #pragma unroll
         for (int c = 0; c < NCH; ++c) acc[s][c] = T(0);
-    const T* Xs[SB];
+    const T* Xs[SB];  // states past the end read the last valid state
 #pragma unroll
     for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
 
-#pragma unroll 2
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-        const int g = pt_g[p];
-        T tv[NCH];
+    // software pipeline: the grid index and table values of the next point are in
+    // flight while the states are gathered at the current one, so each step waits
+    // for one memory latency instead of two dependent ones
+    int p = p0 + threadIdx.x;
+    int g = 0;
+    T tv[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) tv[c] = T(0);
+    if (p < p1) {
+        g = pt_g[p];
 #pragma unroll
         for (int c = 0; c < NCH; ++c) tv[c] = tab[(long long)c * npts + p];
+    }
+#pragma unroll 2
+    for (; p < p1; p += blockDim.x) {
+        const int pn = p + blockDim.x;
+        int gn = 0;
+        T tn[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) tn[c] = T(0);
+        if (pn < p1) {
+            gn = pt_g[pn];
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) tn[c] = tab[(long long)c * npts + pn];
+        }
 #pragma unroll
         for (int s = 0; s < SB; ++s) {
             const T v = Xs[s][g];
 #pragma unroll
             for (int c = 0; c < NCH; ++c) acc[s][c] += tv[c] * v;
         }
+        g = gn;
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) tv[c] = tn[c];
     }
     // block reduction: warp shuffles, then one value per warp through shared memory
     __shared__ T red[8][SB * NCH];
@@ -233,89 +258,154 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
             T v = acc[s][c];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) red[warp][s * NCH + c] = v;
+            if (lane == 0) red[warp][c * SB + s] = v;
         }
     __syncthreads();
     const int nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < SB * NCH; i += blockDim.x) {
         T v = T(0);
         for (int w = 0; w < nw; ++w) v += red[w][i];
-        const int s = i / NCH, c = i % NCH;
+        const int c = i / SB, s = i % SB;
         if (s0 + s < ns)
-            coef[(long long)(s0 + s) * ncoef + atom * NCH + c] = T(ch_scale[atom * NCH + c] * (double)v);
+            coef[(long long)(atom * NCH + c) * ldc + s0 + s] = T(ch_scale[atom * NCH + c] * (double)v);
     }
+}
+
+// States per projection block (or the forced value): the largest of 8 / 4 / 2 / 1
+// that still gives one block per SM. 8 states measured fastest at 32-256 states on
+// 64- and 216-atom cells (16 holds more registers than it saves table reads).
+static int pick_project_sb(int na, int ns, int forced) {
+    if (forced > 0) return forced;
+    for (int sb : {8, 4, 2})
+        if ((long long)na * ((ns + sb - 1) / sb) >= 148) return sb;
+    return 1;
 }
 
 template <typename T, int NCH>
 static void launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X,
-                               long long ldx, T* coef, cudaStream_t st) {
-    const int blocks_per_sb8 = pj.na * ((ns + 7) / 8);
-    if (blocks_per_sb8 >= 2 * 148) {
-        dim3 g(pj.na, (ns + 7) / 8);
-        k_project<T, 8, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
-                                                pj.ch_scale, coef, pj.na * NCH);
-    } else if (pj.na * ((ns + 1) / 2) >= 2 * 148) {
-        dim3 g(pj.na, (ns + 1) / 2);
-        k_project<T, 2, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
-                                                pj.ch_scale, coef, pj.na * NCH);
-    } else {
-        dim3 g(pj.na, ns);
-        k_project<T, 1, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts,
-                                                pj.ch_scale, coef, pj.na * NCH);
+                               long long ldx, T* coef, long long ldc, int sb, cudaStream_t st) {
+    // register budget: 16 states only with 4 channels, 8 with 8, 4 with 16
+    constexpr int kMaxSb = NCH <= 4 ? 16 : (NCH == 8 ? 8 : 4);
+    sb = std::min(sb, kMaxSb);
+    const dim3 g(pj.na, (ns + sb - 1) / sb);
+#define QG_PROJECT(SBV)                                                                                       \
+    k_project<T, SBV, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts, pj.ch_scale, \
+                                              coef, ldc)
+    switch (sb) {
+        case 16:
+            if constexpr (kMaxSb >= 16) QG_PROJECT(16);
+            break;
+        case 8:
+            if constexpr (kMaxSb >= 8) QG_PROJECT(8);
+            break;
+        case 4: QG_PROJECT(4); break;
+        case 2: QG_PROJECT(2); break;
+        default: QG_PROJECT(1); break;
     }
+#undef QG_PROJECT
 }
 
 template <typename T>
-static int launch_project(const DevProjectors& pj, int ns, const T* X, long long ldx, T* coef,
-                          cudaStream_t st) {
+static int launch_project(const DevProjectors& pj, int ns, const T* X, long long ldx, T* coef, long long ldc,
+                          int forced_sb, cudaStream_t st) {
     const T* tab;
     if constexpr (sizeof(T) == 8) tab = reinterpret_cast<const T*>(pj.tab_d);
     else tab = reinterpret_cast<const T*>(pj.tab_f);
+    const int sb = pick_project_sb(pj.na, ns, forced_sb);
     switch (pj.nch) {
-        case 4: launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, st); break;
-        case 8: launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, st); break;
-        case 16: launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, st); break;
+        case 4: launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
+        case 8: launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
+        case 16: launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
         default: return QG_ERR_UNSUPPORTED;
     }
     return QG_OK;
 }
 
-// Nonlocal scatter over all states, one thread per grid point: for each group
-// of SG states it adds sum_{entries e of g} sum_ch val[e][ch] * coef[s][atom_e, ch]
-// to HX[s][g]. The point's entries and the few atoms' coefficients a block
-// touches stay in L1 across the groups.
-template <typename T, int SG, int NCH>
-__global__ void __launch_bounds__(256) k_scatter_all(T* __restrict__ HX, long long ldhx, int ns, long long N,
+// 16-byte vector of T (the unit the scatter reads the coefficients in).
+template <typename T> struct Vec16;
+template <> struct Vec16<double> {
+    using type = double2;
+    static constexpr int n = 2;
+    static __device__ __forceinline__ double at(const double2& v, int i) { return i == 0 ? v.x : v.y; }
+};
+template <> struct Vec16<float> {
+    using type = float4;
+    static constexpr int n = 4;
+    static __device__ __forceinline__ float at(const float4& v, int i) {
+        return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+    }
+};
+
+// Nonlocal scatter over all states, one thread per grid point. The point's first
+// KMAX entries (their coefficient rows and NCH table values) stay in registers for
+// all state groups; for each group of SG states every entry adds
+// sum_ch val[ch] * coef[atom, ch][s0 .. s0+SG), read as 16-byte vectors (the lanes of
+// a warp mostly share the entry's atom, so these are broadcast loads from L1).
+// Entries past KMAX (points inside more than KMAX spheres) are read from memory in
+// the same order, so the sum per point and state is the same as one loop over all.
+template <typename T, int SG, int NCH, int KMAX>
+__global__ void __launch_bounds__(256, SG <= 4 ? 3 : 2) k_scatter_all(T* __restrict__ HX, long long ldhx, int ns, long long N,
                                                      const int* __restrict__ row,
                                                      const int* __restrict__ ent_atom,
                                                      const T* __restrict__ ent_val,
-                                                     const T* __restrict__ coef, int ncoef) {
+                                                     const T* __restrict__ coef, long long ldc) {
+    using V = typename Vec16<T>::type;
+    constexpr int VN = Vec16<T>::n;
+    static_assert(SG % VN == 0, "state group must be whole vectors");
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= N) return;
-    const int e0 = row[g], e1 = row[g + 1];
-    if (e0 == e1) return;
+    const int e0 = row[g], ne = row[g + 1] - e0;
+    if (ne == 0) return;
+    int cb[KMAX];  // first coefficient row of the entry's atom
+    T v[KMAX][NCH];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        cb[k] = 0;
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) v[k][c] = T(0);
+        if (k < ne) {
+            cb[k] = __ldg(&ent_atom[e0 + k]) * NCH;
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) v[k][c] = __ldg(&ent_val[(long long)(e0 + k) * NCH + c]);
+        }
+    }
     for (int s0 = 0; s0 < ns; s0 += SG) {
+        T acc[SG];
+#pragma unroll
+        for (int s = 0; s < SG; ++s) acc[s] = T(0);
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            if (k < ne) {
+#pragma unroll
+                for (int c = 0; c < NCH; ++c) {
+                    const V* cp = reinterpret_cast<const V*>(coef + (long long)(cb[k] + c) * ldc + s0);
+#pragma unroll
+                    for (int j = 0; j < SG / VN; ++j) {
+                        const V w = __ldg(cp + j);
+#pragma unroll
+                        for (int i = 0; i < VN; ++i) acc[j * VN + i] += v[k][c] * Vec16<T>::at(w, i);
+                    }
+                }
+            }
+        }
+        for (int e = e0 + KMAX; e < e0 + ne; ++e) {
+            const T* ce = coef + (long long)__ldg(&ent_atom[e]) * NCH * ldc;
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+                const T vc = __ldg(&ent_val[(long long)e * NCH + c]);
+                const V* cp = reinterpret_cast<const V*>(ce + (long long)c * ldc + s0);
+#pragma unroll
+                for (int j = 0; j < SG / VN; ++j) {
+                    const V w = __ldg(cp + j);
+#pragma unroll
+                    for (int i = 0; i < VN; ++i) acc[j * VN + i] += vc * Vec16<T>::at(w, i);
+                }
+            }
+        }
         const int gn = min(SG, ns - s0);
         T h[SG];
 #pragma unroll
         for (int s = 0; s < SG; ++s) h[s] = (s < gn) ? HX[(long long)(s0 + s) * ldhx + g] : T(0);
-        T acc[SG];
-#pragma unroll
-        for (int s = 0; s < SG; ++s) acc[s] = T(0);
-        const T* cg = coef + (long long)s0 * ncoef;
-        for (int e = e0; e < e1; ++e) {
-            const int base = __ldg(&ent_atom[e]) * NCH;
-            T v[NCH];
-#pragma unroll
-            for (int c = 0; c < NCH; ++c) v[c] = __ldg(&ent_val[(long long)e * NCH + c]);
-#pragma unroll
-            for (int s = 0; s < SG; ++s) {
-                if (s < gn) {
-#pragma unroll
-                    for (int c = 0; c < NCH; ++c) acc[s] += v[c] * __ldg(&cg[s * ncoef + base + c]);
-                }
-            }
-        }
 #pragma unroll
         for (int s = 0; s < SG; ++s)
             if (s < gn) HX[(long long)(s0 + s) * ldhx + g] = h[s] + acc[s];
@@ -324,23 +414,27 @@ __global__ void __launch_bounds__(256) k_scatter_all(T* __restrict__ HX, long lo
 
 template <typename T, int NCH>
 static int launch_scatter_all_nch(const DevProjectors& pj, T* HX, long long ldhx, int ns, long long N,
-                                  const T* coef, cudaStream_t st) {
-    constexpr int SG = 8;
+                                  const T* coef, long long ldc, int sg, cudaStream_t st) {
+    constexpr int KMAX = NCH <= 4 ? 3 : (NCH == 8 ? 2 : 1);
     const T* ev;
     if constexpr (sizeof(T) == 8) ev = reinterpret_cast<const T*>(pj.ent_val_d);
     else ev = reinterpret_cast<const T*>(pj.ent_val_f);
-    k_scatter_all<T, SG, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(HX, ldhx, ns, N, pj.row, pj.ent_atom,
-                                                                           ev, coef, pj.na * NCH);
+    const unsigned grid = (unsigned)((N + 255) / 256);
+    if (sg == 4)
+        k_scatter_all<T, 4, NCH, KMAX><<<grid, 256, 0, st>>>(HX, ldhx, ns, N, pj.row, pj.ent_atom, ev, coef, ldc);
+    else
+        k_scatter_all<T, 8, NCH, KMAX><<<grid, 256, 0, st>>>(HX, ldhx, ns, N, pj.row, pj.ent_atom, ev, coef, ldc);
     return QG_OK;
 }
 
 template <typename T>
 static int launch_scatter_all(const DevProjectors& pj, T* HX, long long ldhx, int ns, long long N, const T* coef,
-                              cudaStream_t st) {
+                              long long ldc, int forced_sg, cudaStream_t st) {
+    const int sg = forced_sg == 4 ? 4 : 8;
     switch (pj.nch) {
-        case 4: return launch_scatter_all_nch<T, 4>(pj, HX, ldhx, ns, N, coef, st);
-        case 8: return launch_scatter_all_nch<T, 8>(pj, HX, ldhx, ns, N, coef, st);
-        case 16: return launch_scatter_all_nch<T, 16>(pj, HX, ldhx, ns, N, coef, st);
+        case 4: return launch_scatter_all_nch<T, 4>(pj, HX, ldhx, ns, N, coef, ldc, sg, st);
+        case 8: return launch_scatter_all_nch<T, 8>(pj, HX, ldhx, ns, N, coef, ldc, sg, st);
+        case 16: return launch_scatter_all_nch<T, 16>(pj, HX, ldhx, ns, N, coef, ldc, sg, st);
         default: return QG_ERR_UNSUPPORTED;
     }
 }
@@ -373,7 +467,7 @@ static int launch_stencil(const HamArgs<T>& a, int nz, cudaStream_t st) {
 size_t coef_scratch_elems(qg_hamiltonian h, int ns) {
     const DevProjectors& pj = h->pj;
     if (pj.na <= 0 || pj.nch <= 0) return 0;
-    return (size_t)ns * pj.na * pj.nch;
+    return (size_t)coef_ld(ns) * pj.na * pj.nch;
 }
 
 template <typename T>
@@ -436,11 +530,11 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
         }
         // projection of all states, persistent stencil + V, then the nonlocal scatter
         if (pt) pt->mark(0, st);
-        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, st));
+        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, st));
         if (pt) pt->mark(1, st);
         QG_TRY(launch_stencil_tma<T>(a, h->order, st));
         if (pt) pt->mark(2, st);
-        QG_TRY(launch_scatter_all<T>(pj, HX, ldhx, ns, N, coef, st));
+        QG_TRY(launch_scatter_all<T>(pj, HX, ldhx, ns, N, coef, coef_ld(ns), h->scatter_sg, st));
         if (pt) pt->mark(-1, st);
         QG_CUDA_TRY(cudaGetLastError());
         return QG_OK;
@@ -448,13 +542,13 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
     // register-window kernel with the nonlocal scatter fused per point
     if (pt) pt->mark(0, st);
     if (nonlocal) {
-        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, st));
+        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, st));
         a.row = pj.row;
         a.ent_atom = pj.ent_atom;
         if constexpr (sizeof(T) == 8) a.ent_val = reinterpret_cast<const T*>(pj.ent_val_d);
         else a.ent_val = reinterpret_cast<const T*>(pj.ent_val_f);
         a.nch = pj.nch;
-        a.ncoef = pj.na * pj.nch;
+        a.ldc = coef_ld(ns);
         a.coef = coef;
     }
     if (pt) pt->mark(1, st);
@@ -622,6 +716,8 @@ void destroy_ham(qg_hamiltonian h) {
     free_projectors(h->pj);
     h->coef.release();
     h->kco.release();
+    if (h->io_in) cudaStreamDestroy(h->io_in);
+    if (h->io_out) cudaStreamDestroy(h->io_out);
     h->xio.release();
     h->hxio.release();
     delete h;
@@ -701,6 +797,69 @@ static int apply_device(qg_hamiltonian h, int ns, const T* X, long long ldx, T* 
     return qg::apply_hamiltonian<T>(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream);
 }
 
+namespace qg {
+
+int host_pipelined_apply(qg_hamiltonian h, int ns, long long row, const double* X, double* HX,
+                         const std::function<int(int, const double*, double*)>& apply) {
+    const size_t bytes = (size_t)ns * row * sizeof(double);
+    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
+    QG_TRY(h->xio.reserve(bytes));
+    QG_TRY(h->hxio.reserve(bytes));
+    if (!h->io_in) QG_CUDA_TRY(cudaStreamCreateWithFlags(&h->io_in, cudaStreamNonBlocking));
+    if (!h->io_out) QG_CUDA_TRY(cudaStreamCreateWithFlags(&h->io_out, cudaStreamNonBlocking));
+    cudaStream_t st = h->ctx->stream;
+    // chunks of states: the copy-in of later chunks (io_in) and the copy-out of
+    // earlier ones (io_out) run on both directions of the host link while the
+    // apply of the current chunk runs on the context stream
+    const int chunk = std::max(1, (ns + kHostChunks - 1) / kHostChunks);
+    const int nchunk = (ns + chunk - 1) / chunk;
+    std::vector<cudaEvent_t> ev(2 * nchunk + 1, nullptr);
+    int rc = QG_OK;
+    for (auto& e : ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) rc = QG_ERR_CUDA;
+    // the copies start after the work already queued on the context stream
+    if (rc == QG_OK && (cudaEventRecord(ev[2 * nchunk], st) != cudaSuccess ||
+                        cudaStreamWaitEvent(h->io_in, ev[2 * nchunk], 0) != cudaSuccess ||
+                        cudaStreamWaitEvent(h->io_out, ev[2 * nchunk], 0) != cudaSuccess))
+        rc = QG_ERR_CUDA;
+    double* xs = h->xio.as<double>();
+    double* hs = h->hxio.as<double>();
+    for (int c = 0; c < nchunk && rc == QG_OK; ++c) {
+        const size_t off = (size_t)c * chunk * row;
+        const size_t cb = (size_t)std::min(chunk, ns - c * chunk) * row * sizeof(double);
+        if (cudaMemcpyAsync(xs + off, X + off, cb, cudaMemcpyHostToDevice, h->io_in) != cudaSuccess ||
+            cudaEventRecord(ev[2 * c], h->io_in) != cudaSuccess)
+            rc = QG_ERR_CUDA;
+    }
+    for (int c = 0; c < nchunk && rc == QG_OK; ++c) {
+        const int nc = std::min(chunk, ns - c * chunk);
+        const size_t off = (size_t)c * chunk * row;
+        if (cudaStreamWaitEvent(st, ev[2 * c], 0) != cudaSuccess) {
+            rc = QG_ERR_CUDA;
+            break;
+        }
+        rc = apply(nc, xs + off, hs + off);
+        if (rc != QG_OK) break;
+        if (cudaEventRecord(ev[2 * c + 1], st) != cudaSuccess ||
+            cudaStreamWaitEvent(h->io_out, ev[2 * c + 1], 0) != cudaSuccess ||
+            cudaMemcpyAsync(HX + off, hs + off, (size_t)nc * row * sizeof(double), cudaMemcpyDeviceToHost,
+                            h->io_out) != cudaSuccess)
+            rc = QG_ERR_CUDA;
+    }
+    const cudaError_t e0 = cudaStreamSynchronize(h->io_in);
+    const cudaError_t e1 = cudaStreamSynchronize(h->io_out);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc != QG_OK) return rc;
+    QG_CUDA_TRY(e0);
+    QG_CUDA_TRY(e1);
+    QG_CUDA_TRY(e2);
+    return QG_OK;
+}
+
+}  // namespace qg
+
 extern "C" {
 
 int qg_hamiltonian_apply_d(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX,
@@ -738,6 +897,17 @@ int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int plain) {
     return QG_OK;
 }
 
+int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian h, int project_states, int scatter_states) {
+    if (!h) return QG_ERR_INVALID;
+    const bool sb_ok = project_states == 0 || project_states == 1 || project_states == 2 || project_states == 4 ||
+                       project_states == 8 || project_states == 16;
+    const bool sg_ok = scatter_states == 0 || scatter_states == 4 || scatter_states == 8;
+    if (!sb_ok || !sg_ok) return QG_ERR_INVALID;
+    h->proj_sb = project_states;
+    h->scatter_sg = scatter_states;
+    return QG_OK;
+}
+
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian h, int ns) {
     if (!h || ns < 0) return QG_ERR_INVALID;
     if (ns == 0) return 0;
@@ -756,16 +926,9 @@ int qg_hamiltonian_apply_host_d(qg_hamiltonian h, int ns, const double* X, doubl
     if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
     if (ns == 0) return QG_OK;
     const long long N = h->N();
-    const size_t bytes = (size_t)ns * N * sizeof(double);
-    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
-    QG_TRY(h->xio.reserve(bytes));
-    QG_TRY(h->hxio.reserve(bytes));
-    cudaStream_t st = h->ctx->stream;
-    QG_CUDA_TRY(cudaMemcpyAsync(h->xio.ptr, X, bytes, cudaMemcpyHostToDevice, st));
-    QG_TRY(apply_device<double>(h, ns, h->xio.as<double>(), N, h->hxio.as<double>(), N));
-    QG_CUDA_TRY(cudaMemcpyAsync(HX, h->hxio.ptr, bytes, cudaMemcpyDeviceToHost, st));
-    QG_CUDA_TRY(cudaStreamSynchronize(st));
-    return QG_OK;
+    return qg::host_pipelined_apply(h, ns, N, X, HX, [&](int nc, const double* xd, double* hd) {
+        return apply_device<double>(h, nc, xd, N, hd, N);
+    });
 }
 
 }  // extern "C"

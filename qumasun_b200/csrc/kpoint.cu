@@ -439,17 +439,10 @@ int qg_hamiltonian_apply_timed_z(qg_hamiltonian h, int ns, const double* X, long
 int qg_hamiltonian_apply_host_z(qg_hamiltonian h, int ns, const double* X, double* HX) {
     if (!h || ns < 0 || (ns > 0 && (!X || !HX))) return QG_ERR_INVALID;
     if (ns == 0) return QG_OK;
-    const long long N = h->N();
-    const size_t bytes = (size_t)ns * 2 * N * sizeof(double);
-    QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
-    QG_TRY(h->xio.reserve(bytes));
-    QG_TRY(h->hxio.reserve(bytes));
-    cudaStream_t st = h->ctx->stream;
-    QG_CUDA_TRY(cudaMemcpyAsync(h->xio.ptr, X, bytes, cudaMemcpyHostToDevice, st));
-    QG_TRY(apply_z_checked(h, ns, h->xio.as<double>(), 2 * N, h->hxio.as<double>(), 2 * N));
-    QG_CUDA_TRY(cudaMemcpyAsync(HX, h->hxio.ptr, bytes, cudaMemcpyDeviceToHost, st));
-    QG_CUDA_TRY(cudaStreamSynchronize(st));
-    return QG_OK;
+    const long long N2 = 2 * h->N();
+    return qg::host_pipelined_apply(h, ns, N2, X, HX, [&](int nc, const double* xd, double* hd) {
+        return apply_z_checked(h, nc, xd, N2, hd, N2);
+    });
 }
 
 }  // extern "C"

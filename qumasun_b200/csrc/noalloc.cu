@@ -16,7 +16,7 @@
 
 namespace {
 
-// Projector-coefficient scratch, [ns][n_atoms * n_channels] doubles, for every
+// Projector-coefficient scratch, [n_atoms * n_channels][ns rounded up to 16] doubles, for every
 // no-allocation call on a device. 2^19 doubles = 4 MiB per device that loads
 // the library, held until the process exits.
 constexpr size_t kNoAllocCoefMax = size_t(1) << 19;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <vector>
 
 #include "../../include/qumasun_b200.h"
@@ -108,8 +109,11 @@ struct qg_hamiltonian_s {
     DevBuf coef;      // projector coefficients E*dV*<p|psi>, [ns][na*nch]
     DevBuf xio, hxio; // staging for the host-buffer entry point
     DevBuf kco;       // per-k-point stencil coefficients of a multi-k apply
+    cudaStream_t io_in = nullptr, io_out = nullptr;  // copy streams of the host-buffer entry points
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
+    int proj_sb = 0;     // states per projection block (0: chosen per launch)
+    int scatter_sg = 0;  // states per scatter group (0: 8)
     qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
     qg_learned learned = nullptr;           // network of precond = 2 (qg_hamiltonian_set_learned)
     double learned_vscale = 1.0;
@@ -149,7 +153,19 @@ struct PhaseTimer {
     }
 };
 
-// Elements of projector-coefficient scratch ([ns][n_atoms * n_channels]) one apply of ns states needs.
+// Host-buffer apply, pipelined over kHostChunks chunks of states through the
+// staging buffers h->xio / h->hxio (hamiltonian.cu). Each state is `row` doubles;
+// apply(nc, x_dev, hx_dev) queues the operator on the context stream.
+constexpr int kHostChunks = 8;
+int host_pipelined_apply(qg_hamiltonian h, int ns, long long row, const double* X, double* HX,
+                         const std::function<int(int, const double*, double*)>& apply);
+
+// Row length of the channel-major projector coefficients [na * nch][ld]: the state
+// count rounded up to 16, so every row starts 128-byte aligned and the scatter's
+// 16-byte loads of a state group never leave the row.
+inline long long coef_ld(int ns) { return (ns + 15) / 16 * 16; }
+
+// Elements of projector-coefficient scratch ([n_atoms * n_channels][coef_ld(ns)]) one apply of ns states needs.
 size_t coef_scratch_elems(qg_hamiltonian h, int ns);
 
 template <typename T>

@@ -22,8 +22,8 @@ struct HamArgs {
     const int* ent_atom;
     const T* ent_val;
     int nch;
-    int ncoef;       // na * nch
-    const T* coef;   // [ns][ncoef]
+    long long ldc;   // coefficient row length (states, padded to 16)
+    const T* coef;   // [na * nch][ldc]
     int* err;        // device status word: nonzero after a bounded wait gave up
     // complex (k-point) states: the imaginary part of a state starts xim (hxim)
     // elements after its real part; dx/dy/dz are the 8th-order first-derivative

@@ -50,6 +50,40 @@ def test_fp64_and_fp32_match_oracle_diamond8(cuda_ctx, order):
     assert rel_per_state(gpu_apply(cuda_ctx, cell, X.astype(np.float32), order, "f32"), ref).max() < TOL32
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(grid=(12, 12, 12), a0=4.4)], ids=["diamond8", "wrap"])
+def test_nonlocal_blocking_gives_identical_results(cuda_ctx, kw):
+    """Every projection / scatter state blocking (and the register-window kernel,
+    which reads the same channel-major coefficients) gives the same bits; the wrap
+    cell has points inside up to 10 projector spheres, past the scatter's register
+    cache of 4 entries."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(**kw)
+    X = initial_states(21, cell.N, seed=17)  # ragged against every state group
+    H = Hamiltonian(cuda_ctx, cell)
+    for dt in (torch.float64, torch.float32):
+        Xd = torch.from_numpy(X).to("cuda", dt)
+        H.set_nonlocal_blocking(0, 0)
+        base = H.apply(Xd).cpu().numpy()
+        for sb in (1, 2, 4, 8, 16):
+            for sg in (4, 8):
+                H.set_nonlocal_blocking(sb, sg)
+                np.testing.assert_array_equal(H.apply(Xd).cpu().numpy(), base)
+        H.set_nonlocal_blocking(0, 0)
+        H.set_stencil_kernel(True)
+        plain = H.apply(Xd).cpu().numpy()
+        H.set_stencil_kernel(False)
+        ref = O.hamiltonian_apply(cell, X)
+        tol = TOL64 if dt == torch.float64 else TOL32
+        assert rel_per_state(base, ref).max() < tol
+        assert rel_per_state(plain, ref).max() < tol
+    with pytest.raises(Exception):
+        H.set_nonlocal_blocking(3, 0)
+    with pytest.raises(Exception):
+        H.set_nonlocal_blocking(0, 16)
+    H.close()
+
+
 def test_displaced_cell_no_nonlocal_and_no_potential(cuda_ctx):
     for kw in [dict(grid=(24, 20, 16), displacement=0.3, seed=5),
                dict(grid=(16, 16, 16), nonlocal_on=False),
@@ -80,10 +114,14 @@ def test_strided_states_and_empty_batch(cuda_ctx):
     H.close()
 
 
-def test_host_entry_point_matches_device(cuda_ctx):
+@pytest.mark.parametrize("ns", [1, 4, 13])
+def test_host_entry_point_matches_device(cuda_ctx, ns):
+    """The host-buffer entry point copies in, applies and copies out in chunks of
+    states on separate streams; ragged last chunks included, it equals the device
+    apply bit for bit."""
     from qumasun_b200 import Hamiltonian
     cell = build_cell(grid=(20, 20, 20))
-    X = initial_states(4, cell.N, seed=6)
+    X = initial_states(ns, cell.N, seed=6)
     H = Hamiltonian(cuda_ctx, cell)
     HXh = H.apply_host(X)
     H.close()
