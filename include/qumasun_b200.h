@@ -323,9 +323,10 @@ int qg_sygv_small_batched_d(qg_context ctx, int batch, int k, const double* A, c
  * where the shape and alignment allow (default), 1 = always the
  * register-window kernel (any shape). Both compute the same operator. */
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int plain);
-/* Tuning of the nonlocal passes of the real apply: states per projection block
- * (1, 2, 4, 8 or 16) and per scatter group (4 or 8); 0 = the engine's choice.
- * The result does not depend on either (same sums in the same order). */
+/* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
+ * complex states use at most 4) and per scatter group of the real apply (4 or 8);
+ * 0 = the engine's choice. The result does not depend on either (same sums in the
+ * same order). */
 int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian ham, int project_states, int scatter_states);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);

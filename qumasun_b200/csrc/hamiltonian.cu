@@ -470,6 +470,12 @@ size_t coef_scratch_elems(qg_hamiltonian h, int ns) {
     return (size_t)coef_ld(ns) * pj.na * pj.nch;
 }
 
+size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk) {
+    const DevProjectors& pj = h->pj;
+    if (pj.na <= 0 || pj.nch <= 0) return 0;
+    return (size_t)2 * nk * coef_ld(nsk) * pj.na * pj.nch;
+}
+
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
                       T* coef, cudaStream_t st, PhaseTimer* pt) {

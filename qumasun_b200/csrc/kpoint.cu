@@ -5,7 +5,7 @@
 //   (mCreateProjectorRadialOnBlock, PseudoPotOperator_kpoint_v2.h:287-420; ProjectionPP :2581-2700).
 // States are split complex, one state = {re[N], im[N]} (lobpcg_z_multi_mpi.h:1005-1012).
 // Three launches for a block of states, as on the real path:
-//   k_project_z     c[s][a,ch] = E dV sum_p P(p) u_s(g(p))          (no conjugate, mInnerNonlocalPsi_v2)
+//   k_project_z     c[k][a,ch][s] = E dV sum_p P(p) u_s(g(p))       (no conjugate, mInnerNonlocalPsi_v2)
 //   k_stencil_tma   V u - 1/2 (Lap + 2i g.grad - g^2) u, both parts of a plane staged together
 //                   (stencil_tma.cu, NC = 2); any other shape runs k_kpoint_plain
 //   k_scatter_all_z Hu[s][g] += sum_entries conj(P) c                 (the scatter of ProjectionPP)
@@ -51,14 +51,17 @@ __global__ void k_bloch_tables(const double* __restrict__ tab, const int* __rest
 
 // Complex gather-contraction: one block per (atom, k-point, group of SB states).
 // c = sum_p (tr + i ti)(ur + i ui), scaled by E dV per channel; the states of k-point k
-// start at X + k*ldk, the Bloch tables of k at ztab + k*zstride.
+// start at X + k*ldk, the Bloch tables of k at ztab + k*zstride. The coefficients are
+// stored channel-major per k-point, {re, im} pairs at
+// coef[((k * na * NCH + atom * NCH + ch) * ldc + s) * 2], so the scatter reads the
+// states of one (k, atom, channel) as contiguous 16-byte pairs.
 template <int SB, int NCH>
 __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X, long long ldx, long long ldk,
                                                    long long xim, int nsk, int groups,
                                                    const int* __restrict__ atom_off, const int* __restrict__ pt_g,
                                                    const double* __restrict__ ztab, long long zstride, long long npts,
                                                    const double* __restrict__ ch_scale, double* __restrict__ coef,
-                                                   int ncoef) {
+                                                   int ncoef, long long ldc) {
     const int atom = blockIdx.x;
     const int k = blockIdx.y / groups;
     const int s0 = (blockIdx.y - k * groups) * SB;
@@ -115,57 +118,88 @@ __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X,
         for (int w = 0; w < nw; ++w) v += red[w][i];
         const int sc = i >> 1, s = sc / NCH, c = sc % NCH;
         if (s0 + s < nsk)
-            coef[(((long long)k * nsk + s0 + s) * ncoef + atom * NCH + c) * 2 + (i & 1)] = ch_scale[atom * NCH + c] * v;
+            coef[(((long long)k * ncoef + atom * NCH + c) * ldc + s0 + s) * 2 + (i & 1)] =
+                ch_scale[atom * NCH + c] * v;
     }
 }
 
-// Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[s][a_e, ch],
-// k-point by k-point (tables zent + k*zstride, states of k at HX + k*ldk).
-template <int SG, int NCH>
-__global__ void __launch_bounds__(256) k_scatter_all_z(double* __restrict__ HX, long long ldhx, long long ldk,
+// Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[a_e, ch][s],
+// k-point by k-point (tables zent + k*zstride, states of k at HX + k*ldk). The point's
+// first KMAX entries keep their coefficient row in registers, and per k-point their
+// Bloch-phase values; the coefficients of a state group are read as {re, im} 16-byte
+// pairs (broadcasts across the warp). Entries past KMAX are read from memory in the
+// same order.
+template <int SG, int NCH, int KMAX>
+__global__ void __launch_bounds__(256, 2) k_scatter_all_z(double* __restrict__ HX, long long ldhx, long long ldk,
                                                        long long hxim, int nk, int nsk, long long N,
                                                        const int* __restrict__ row, const int* __restrict__ ent_atom,
                                                        const double* __restrict__ zent, long long zstride,
-                                                       const double* __restrict__ coef, int ncoef) {
+                                                       const double* __restrict__ coef, int ncoef, long long ldc) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= N) return;
-    const int e0 = row[g], e1 = row[g + 1];
-    if (e0 == e1) return;
+    const int e0 = row[g], ne = row[g + 1] - e0;
+    if (ne == 0) return;
+    int cb[KMAX];
+#pragma unroll
+    for (int kk = 0; kk < KMAX; ++kk) cb[kk] = kk < ne ? __ldg(&ent_atom[e0 + kk]) * NCH : 0;
     for (int k = 0; k < nk; ++k) {
         const double* zk = zent + (long long)k * zstride;
+        const double2* ck = reinterpret_cast<const double2*>(coef) + (long long)k * ncoef * ldc;
+        double vr[KMAX][NCH], vi[KMAX][NCH];
+#pragma unroll
+        for (int kk = 0; kk < KMAX; ++kk)
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+                vr[kk][c] = kk < ne ? __ldg(&zk[((long long)(e0 + kk) * NCH + c) * 2]) : 0.0;
+                vi[kk][c] = kk < ne ? __ldg(&zk[((long long)(e0 + kk) * NCH + c) * 2 + 1]) : 0.0;
+            }
         for (int s0 = 0; s0 < nsk; s0 += SG) {
             const int gn = min(SG, nsk - s0);
             double accr[SG], acci[SG];
 #pragma unroll
             for (int s = 0; s < SG; ++s) accr[s] = acci[s] = 0.0;
-            const double* cg = coef + ((long long)k * nsk + s0) * ncoef * 2;
-            for (int e = e0; e < e1; ++e) {
-                const int base = __ldg(&ent_atom[e]) * NCH;
-                double vr[NCH], vi[NCH];
 #pragma unroll
-                for (int c = 0; c < NCH; ++c) {
-                    vr[c] = __ldg(&zk[((long long)e * NCH + c) * 2]);
-                    vi[c] = __ldg(&zk[((long long)e * NCH + c) * 2 + 1]);
-                }
+            for (int kk = 0; kk < KMAX; ++kk) {
+                if (kk < ne) {
 #pragma unroll
-                for (int s = 0; s < SG; ++s) {
-                    if (s < gn) {
+                    for (int c = 0; c < NCH; ++c) {
+                        const double2* cp = ck + (long long)(cb[kk] + c) * ldc + s0;
 #pragma unroll
-                        for (int c = 0; c < NCH; ++c) {
-                            const double cr = __ldg(&cg[((long long)s * ncoef + base + c) * 2]);
-                            const double ci = __ldg(&cg[((long long)s * ncoef + base + c) * 2 + 1]);
-                            accr[s] += vr[c] * cr + vi[c] * ci;
-                            acci[s] += vr[c] * ci - vi[c] * cr;
+                        for (int s = 0; s < SG; ++s) {
+                            const double2 w = __ldg(cp + s);
+                            accr[s] += vr[kk][c] * w.x + vi[kk][c] * w.y;
+                            acci[s] += vr[kk][c] * w.y - vi[kk][c] * w.x;
                         }
                     }
                 }
             }
+            for (int e = e0 + KMAX; e < e0 + ne; ++e) {
+                const int base = __ldg(&ent_atom[e]) * NCH;
+#pragma unroll
+                for (int c = 0; c < NCH; ++c) {
+                    const double er = __ldg(&zk[((long long)e * NCH + c) * 2]);
+                    const double ei = __ldg(&zk[((long long)e * NCH + c) * 2 + 1]);
+                    const double2* cp = ck + (long long)(base + c) * ldc + s0;
+#pragma unroll
+                    for (int s = 0; s < SG; ++s) {
+                        const double2 w = __ldg(cp + s);
+                        accr[s] += er * w.x + ei * w.y;
+                        acci[s] += er * w.y - ei * w.x;
+                    }
+                }
+            }
+            double hr[SG], hi[SG];
+            double* hb = HX + (long long)k * ldk + (long long)s0 * ldhx + g;
+#pragma unroll
+            for (int s = 0; s < SG; ++s) {
+                hr[s] = s < gn ? hb[(long long)s * ldhx] : 0.0;
+                hi[s] = s < gn ? hb[(long long)s * ldhx + hxim] : 0.0;
+            }
 #pragma unroll
             for (int s = 0; s < SG; ++s)
                 if (s < gn) {
-                    double* hr = HX + (long long)k * ldk + (long long)(s0 + s) * ldhx + g;
-                    hr[0] += accr[s];
-                    hr[hxim] += acci[s];
+                    hb[(long long)s * ldhx] = hr[s] + accr[s];
+                    hb[(long long)s * ldhx + hxim] = hi[s] + acci[s];
                 }
         }
     }
@@ -225,30 +259,44 @@ __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<double> a) {
 
 template <int NCH>
 void launch_project_z_nch(const DevProjectors& pj, int nk, int nsk, const double* X, long long ldx, long long ldk,
-                          long long xim, double* coef, cudaStream_t st) {
+                          long long xim, double* coef, int forced_sb, cudaStream_t st) {
+    // states per block: the largest of 4 / 2 / 1 (within the register budget of NCH
+    // channels) that still gives one block per SM
+    constexpr int kMaxSb = NCH <= 4 ? 4 : (NCH == 8 ? 2 : 1);
     const long long zstride = 2LL * pj.nch * pj.npts;
-    if (pj.na * nk * ((nsk + 3) / 4) >= 2 * 148) {
-        const int groups = (nsk + 3) / 4;
-        dim3 g(pj.na, nk * groups);
-        k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
-                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
-    } else if (pj.na * nk * ((nsk + 1) / 2) >= 2 * 148) {
-        const int groups = (nsk + 1) / 2;
-        dim3 g(pj.na, nk * groups);
-        k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
-                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
+    const long long ldc = coef_ld(nsk);
+    int sb = 1;
+    if (forced_sb > 0) {
+        sb = std::min(forced_sb, kMaxSb);
     } else {
-        dim3 g(pj.na, nk * nsk);
-        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, nsk, pj.atom_off, pj.pt_g, pj.ztab, zstride,
-                                               pj.npts, pj.ch_scale, coef, pj.na * NCH);
+        for (int c : {4, 2})
+            if (c <= kMaxSb && (long long)pj.na * nk * ((nsk + c - 1) / c) >= 148) {
+                sb = c;
+                break;
+            }
     }
+    const int groups = (nsk + sb - 1) / sb;
+    const dim3 g(pj.na, nk * groups);
+    if (sb == 4) {
+        if constexpr (kMaxSb >= 4)
+            k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab,
+                                                   zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
+    } else if (sb == 2) {
+        if constexpr (kMaxSb >= 2)
+            k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab,
+                                                   zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
+    } else
+        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
+                                               pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
 }
 
 template <int NCH>
 void launch_scatter_z_nch(const DevProjectors& pj, int nk, int nsk, double* HX, long long ldhx, long long ldk,
                           long long hxim, long long N, const double* coef, cudaStream_t st) {
-    k_scatter_all_z<4, NCH><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
-        HX, ldhx, ldk, hxim, nk, nsk, N, pj.row, pj.ent_atom, pj.zent, 2LL * pj.nch * pj.nent, coef, pj.na * NCH);
+    constexpr int KMAX = NCH <= 4 ? 3 : (NCH == 8 ? 2 : 1);
+    k_scatter_all_z<4, NCH, KMAX><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        HX, ldhx, ldk, hxim, nk, nsk, N, pj.row, pj.ent_atom, pj.zent, 2LL * pj.nch * pj.nent, coef, pj.na * NCH,
+        coef_ld(nsk));
 }
 
 // Bloch-phase tables for the k-vectors kv (3 per k-point), rebuilt when they change.
@@ -341,9 +389,9 @@ int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, co
     if (nonlocal) {
         QG_TRY(ensure_bloch_tables(h, nk, kv, st));
         switch (pj.nch) {
-            case 4: launch_project_z_nch<4>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
-            case 8: launch_project_z_nch<8>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
-            case 16: launch_project_z_nch<16>(pj, nk, nsk, X, ldx, ldk, N, coef, st); break;
+            case 4: launch_project_z_nch<4>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
+            case 8: launch_project_z_nch<8>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
+            case 16: launch_project_z_nch<16>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
             default: return QG_ERR_UNSUPPORTED;
         }
     }
@@ -386,7 +434,7 @@ int apply_z_checked(qg_hamiltonian h, int ns, const double* X, long long ldx, do
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     double* coef = nullptr;
     if (h->pj.na > 0) {
-        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, ns) * sizeof(double)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems_z(h, 1, ns) * sizeof(double)));
         coef = h->coef.as<double>();
     }
     return qg::apply_hamiltonian_z(h, ns, X, ldx, HX, ldhx, coef, h->ctx->stream);
@@ -407,7 +455,7 @@ int qg_hamiltonian_apply_zk(qg_hamiltonian h, int nk, const double* kvecs, int n
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     double* coef = nullptr;
     if (h->pj.na > 0) {
-        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, nk * nsk) * sizeof(double)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems_z(h, nk, nsk) * sizeof(double)));
         coef = h->coef.as<double>();
     }
     return qg::apply_hamiltonian_zk(h, nk, kvecs, nsk, X, ldx, ldk, HX, ldhx, ldkh, coef, h->ctx->stream);
@@ -426,7 +474,7 @@ int qg_hamiltonian_apply_timed_z(qg_hamiltonian h, int ns, const double* X, long
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     double* coef = nullptr;
     if (h->pj.na > 0) {
-        QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, ns) * sizeof(double)));
+        QG_TRY(h->coef.reserve(qg::coef_scratch_elems_z(h, 1, ns) * sizeof(double)));
         coef = h->coef.as<double>();
     }
     qg::PhaseTimer pt;

@@ -349,7 +349,8 @@ struct Solver {
             lwork = std::max(lwork, lw2);
             QG_TRY(work.reserve((size_t)std::max(lwork, 1) * sizeof(cuDoubleComplex)));
         }
-        QG_TRY(h->coef.reserve((size_t)c * qg::coef_scratch_elems(h, n) * sizeof(double)));
+        QG_TRY(h->coef.reserve((c == 1 ? qg::coef_scratch_elems(h, n) : qg::coef_scratch_elems_z(h, 1, n)) *
+                               sizeof(double)));
         if (mixed) QG_TRY(mg.setup(N, (int)g3));
         return QG_OK;
     }
@@ -845,7 +846,7 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         s.lwork = std::max(lw1, lw2);
         QG_TRY(s.work.reserve((size_t)std::max(s.lwork, 1) * sizeof(cuDoubleComplex)));
     }
-    QG_TRY(h->coef.reserve(2 * qg::coef_scratch_elems(h, nt) * sizeof(double)));
+    QG_TRY(h->coef.reserve(qg::coef_scratch_elems_z(h, nk, nb) * sizeof(double)));
     const size_t blk_bytes = blk * sizeof(double);
     const bool first = opt->first_call != 0;
     const double tol = opt->tol > 0 ? opt->tol : 1.0e-10;

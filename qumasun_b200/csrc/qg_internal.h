@@ -167,6 +167,9 @@ inline long long coef_ld(int ns) { return (ns + 15) / 16 * 16; }
 
 // Elements of projector-coefficient scratch ([n_atoms * n_channels][coef_ld(ns)]) one apply of ns states needs.
 size_t coef_scratch_elems(qg_hamiltonian h, int ns);
+// Doubles of complex coefficient scratch ([nk][n_atoms * n_channels][coef_ld(nsk)] {re, im})
+// one k-point apply of nk k-points x nsk states needs.
+size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk);
 
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
