@@ -324,10 +324,15 @@ int qg_sygv_small_batched_d(qg_context ctx, int batch, int k, const double* A, c
  * register-window kernel (any shape). Both compute the same operator. */
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int plain);
 /* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
- * complex states use at most 4) and per scatter group of the real apply (4 or 8);
- * 0 = the engine's choice. The result does not depend on either (same sums in the
- * same order). */
-int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian ham, int project_states, int scatter_states);
+ * complex states use at most 4), states per scatter group of the real apply (4 or
+ * 8), and blocks per atom in the projection (1-8, one thread-block cluster; the
+ * engine's choice follows the cell alone: one per 8192 sphere points, doubled for
+ * cells of at most 16 atoms); 0 = the
+ * engine's choice. The block sizes do not change the result (same sums in the same
+ * order); the parts per atom change the summation order of the projections (last
+ * bits only), and the engine's choice never depends on the number of states. */
+int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian ham, int project_states, int scatter_states,
+                                         int project_parts);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
 

@@ -22,9 +22,13 @@
 #include <functional>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "qg_internal.h"
 #include "stencil_common.cuh"
 #include "precond.h"
+
+namespace cg = cooperative_groups;
 
 namespace qg {
 
@@ -191,7 +195,14 @@ __global__ void __launch_bounds__(1024) k_hamiltonian(const HamArgs<T> a) {
     }
 }
 
-// Gather-contraction of the projectors: one block per (atom, group of SB states).
+// Gather-contraction of the projectors. `chunks` blocks serve one (atom, group of
+// SB states) as a thread-block cluster: block r sums the r-th contiguous part of the
+// atom's sphere points, the partial sums meet in block 0 through distributed shared
+// memory and are added in rank order. The split depends only on the cell (never on
+// the number of states), so an apply gives the same bits for a state whatever batch
+// it is in. Splitting an atom shortens each block's serial walk over its points
+// (latency-bound for small cells) and keeps all atoms of one state group on the GPU
+// together, so their overlapping spheres are gathered from L2.
 // The coefficients are stored channel-major, coef[(atom * NCH + ch) * ldc + s], so
 // that the scatter reads the states of one (atom, channel) as contiguous vectors.
 template <typename T, int SB, int NCH>
@@ -200,10 +211,14 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
                                                  const int* __restrict__ pt_g,
                                                  const T* __restrict__ tab, long long npts,
                                                  const double* __restrict__ ch_scale,
-                                                 T* __restrict__ coef, long long ldc) {
-    const int atom = blockIdx.x;
+                                                 T* __restrict__ coef, long long ldc, int chunks) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int atom = blockIdx.x / chunks;
     const int s0 = blockIdx.y * SB;
-    const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
+    const int a0 = atom_off[atom], a1 = atom_off[atom + 1];
+    const int len = (a1 - a0 + chunks - 1) / chunks;
+    const int p0 = min(a1, a0 + rank * len), p1 = min(a1, p0 + len);
     T acc[SB][NCH];
 #pragma unroll
     for (int s = 0; s < SB; ++s)
@@ -250,6 +265,7 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
     }
     // block reduction: warp shuffles, then one value per warp through shared memory
     __shared__ T red[8][SB * NCH];
+    __shared__ T part[SB * NCH];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int s = 0; s < SB; ++s)
@@ -265,60 +281,78 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
     for (int i = threadIdx.x; i < SB * NCH; i += blockDim.x) {
         T v = T(0);
         for (int w = 0; w < nw; ++w) v += red[w][i];
-        const int c = i / SB, s = i % SB;
-        if (s0 + s < ns)
-            coef[(long long)(atom * NCH + c) * ldc + s0 + s] = T(ch_scale[atom * NCH + c] * (double)v);
+        part[i] = v;
     }
+    cluster.sync();  // every part's sums are in its block's shared memory
+    if (rank == 0) {
+        for (int i = threadIdx.x; i < SB * NCH; i += blockDim.x) {
+            T v = T(0);
+            for (int r = 0; r < chunks; ++r) v += *cluster.map_shared_rank(&part[i], r);
+            const int c = i / SB, s = i % SB;
+            if (s0 + s < ns)
+                coef[(long long)(atom * NCH + c) * ldc + s0 + s] = T(ch_scale[atom * NCH + c] * (double)v);
+        }
+    }
+    cluster.sync();  // the other parts keep their shared memory until block 0 has read it
 }
 
 // States per projection block (or the forced value): the largest of 8 / 4 / 2 / 1
 // that still gives one block per SM. 8 states measured fastest at 32-256 states on
 // 64- and 216-atom cells (16 holds more registers than it saves table reads).
-static int pick_project_sb(int na, int ns, int forced) {
+static int pick_project_sb(int blocks_per_group, int ns, int forced) {
     if (forced > 0) return forced;
     for (int sb : {8, 4, 2})
-        if ((long long)na * ((ns + sb - 1) / sb) >= 148) return sb;
+        if ((long long)blocks_per_group * ((ns + sb - 1) / sb) >= 148) return sb;
     return 1;
 }
 
 template <typename T, int NCH>
-static void launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X,
-                               long long ldx, T* coef, long long ldc, int sb, cudaStream_t st) {
+static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X, long long ldx, T* coef,
+                              long long ldc, int sb, int parts, cudaStream_t st) {
     // register budget: 16 states only with 4 channels, 8 with 8, 4 with 16
     constexpr int kMaxSb = NCH <= 4 ? 16 : (NCH == 8 ? 8 : 4);
     sb = std::min(sb, kMaxSb);
-    const dim3 g(pj.na, (ns + sb - 1) / sb);
-#define QG_PROJECT(SBV)                                                                                       \
-    k_project<T, SBV, NCH><<<g, 256, 0, st>>>(X, ldx, ns, pj.atom_off, pj.pt_g, tab, pj.npts, pj.ch_scale, \
-                                              coef, ldc)
+    const dim3 g(pj.na * parts, (ns + sb - 1) / sb);
+    cudaError_t e;
+#define QG_PROJECT(SBV)                                                                                              \
+    e = launch_clustered(k_project<T, SBV, NCH>, g, dim3(256), parts, st, X, ldx, ns, pj.atom_off, pj.pt_g, tab, \
+                         pj.npts, pj.ch_scale, coef, ldc, parts)
     switch (sb) {
         case 16:
-            if constexpr (kMaxSb >= 16) QG_PROJECT(16);
-            break;
+            if constexpr (kMaxSb >= 16) {
+                QG_PROJECT(16);
+                break;
+            }
+            [[fallthrough]];
         case 8:
-            if constexpr (kMaxSb >= 8) QG_PROJECT(8);
-            break;
+            if constexpr (kMaxSb >= 8) {
+                QG_PROJECT(8);
+                break;
+            }
+            [[fallthrough]];
         case 4: QG_PROJECT(4); break;
         case 2: QG_PROJECT(2); break;
         default: QG_PROJECT(1); break;
     }
 #undef QG_PROJECT
+    QG_CUDA_TRY(e);
+    return QG_OK;
 }
 
 template <typename T>
 static int launch_project(const DevProjectors& pj, int ns, const T* X, long long ldx, T* coef, long long ldc,
-                          int forced_sb, cudaStream_t st) {
+                          int forced_sb, int forced_parts, cudaStream_t st) {
     const T* tab;
     if constexpr (sizeof(T) == 8) tab = reinterpret_cast<const T*>(pj.tab_d);
     else tab = reinterpret_cast<const T*>(pj.tab_f);
-    const int sb = pick_project_sb(pj.na, ns, forced_sb);
+    const int parts = project_parts(pj, forced_parts);
+    const int sb = pick_project_sb(pj.na * parts, ns, forced_sb);
     switch (pj.nch) {
-        case 4: launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
-        case 8: launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
-        case 16: launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, ldc, sb, st); break;
+        case 4: return launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
+        case 8: return launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
+        case 16: return launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
         default: return QG_ERR_UNSUPPORTED;
     }
-    return QG_OK;
 }
 
 // 16-byte vector of T (the unit the scatter reads the coefficients in).
@@ -536,7 +570,7 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
         }
         // projection of all states, persistent stencil + V, then the nonlocal scatter
         if (pt) pt->mark(0, st);
-        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, st));
+        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, h->proj_parts, st));
         if (pt) pt->mark(1, st);
         QG_TRY(launch_stencil_tma<T>(a, h->order, st));
         if (pt) pt->mark(2, st);
@@ -548,7 +582,7 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
     // register-window kernel with the nonlocal scatter fused per point
     if (pt) pt->mark(0, st);
     if (nonlocal) {
-        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, st));
+        QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, h->proj_parts, st));
         a.row = pj.row;
         a.ent_atom = pj.ent_atom;
         if constexpr (sizeof(T) == 8) a.ent_val = reinterpret_cast<const T*>(pj.ent_val_d);
@@ -700,6 +734,8 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
 
     DevProjectors& pj = h->pj;
     pj.na = na; pj.nch = nch; pj.npts = npts; pj.nent = npts;
+    pj.max_atom_pts = 0;
+    for (int a = 0; a < na; ++a) pj.max_atom_pts = std::max<long long>(pj.max_atom_pts, atom_off[a + 1] - atom_off[a]);
     QG_TRY(upload(&pj.atom_off, atom_off));
     QG_TRY(upload(&pj.pt_g, pt_g));
     QG_TRY(upload(&pj.tab_d, tab_d));
@@ -903,14 +939,17 @@ int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int plain) {
     return QG_OK;
 }
 
-int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian h, int project_states, int scatter_states) {
+int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian h, int project_states, int scatter_states,
+                                         int project_parts) {
     if (!h) return QG_ERR_INVALID;
     const bool sb_ok = project_states == 0 || project_states == 1 || project_states == 2 || project_states == 4 ||
                        project_states == 8 || project_states == 16;
     const bool sg_ok = scatter_states == 0 || scatter_states == 4 || scatter_states == 8;
-    if (!sb_ok || !sg_ok) return QG_ERR_INVALID;
+    const bool pp_ok = project_parts >= 0 && project_parts <= 8;
+    if (!sb_ok || !sg_ok || !pp_ok) return QG_ERR_INVALID;
     h->proj_sb = project_states;
     h->scatter_sg = scatter_states;
+    h->proj_parts = project_parts;
     return QG_OK;
 }
 

@@ -14,8 +14,12 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 #include "qg_internal.h"
 #include "stencil_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace qg {
 namespace {
@@ -55,17 +59,23 @@ __global__ void k_bloch_tables(const double* __restrict__ tab, const int* __rest
 // stored channel-major per k-point, {re, im} pairs at
 // coef[((k * na * NCH + atom * NCH + ch) * ldc + s) * 2], so the scatter reads the
 // states of one (k, atom, channel) as contiguous 16-byte pairs.
+// As on the real path, `parts` blocks (a thread-block cluster) split each atom's
+// points and add their partial sums in rank order through distributed shared memory.
 template <int SB, int NCH>
 __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X, long long ldx, long long ldk,
                                                    long long xim, int nsk, int groups,
                                                    const int* __restrict__ atom_off, const int* __restrict__ pt_g,
                                                    const double* __restrict__ ztab, long long zstride, long long npts,
                                                    const double* __restrict__ ch_scale, double* __restrict__ coef,
-                                                   int ncoef, long long ldc) {
-    const int atom = blockIdx.x;
+                                                   int ncoef, long long ldc, int parts) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int atom = blockIdx.x / parts;
     const int k = blockIdx.y / groups;
     const int s0 = (blockIdx.y - k * groups) * SB;
-    const int p0 = atom_off[atom], p1 = atom_off[atom + 1];
+    const int a0 = atom_off[atom], a1 = atom_off[atom + 1];
+    const int len = (a1 - a0 + parts - 1) / parts;
+    const int p0 = min(a1, a0 + rank * len), p1 = min(a1, p0 + len);
     const double* tab = ztab + (long long)k * zstride;
     double ar[SB][NCH], ai[SB][NCH];
 #pragma unroll
@@ -95,6 +105,7 @@ __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X,
         }
     }
     __shared__ double red[8][2 * SB * NCH];
+    __shared__ double part[2 * SB * NCH];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int s = 0; s < SB; ++s)
@@ -116,11 +127,20 @@ __global__ void __launch_bounds__(256) k_project_z(const double* __restrict__ X,
     for (int i = threadIdx.x; i < 2 * SB * NCH; i += blockDim.x) {
         double v = 0.0;
         for (int w = 0; w < nw; ++w) v += red[w][i];
-        const int sc = i >> 1, s = sc / NCH, c = sc % NCH;
-        if (s0 + s < nsk)
-            coef[(((long long)k * ncoef + atom * NCH + c) * ldc + s0 + s) * 2 + (i & 1)] =
-                ch_scale[atom * NCH + c] * v;
+        part[i] = v;
     }
+    cluster.sync();  // every part's sums are in its block's shared memory
+    if (rank == 0) {
+        for (int i = threadIdx.x; i < 2 * SB * NCH; i += blockDim.x) {
+            double v = 0.0;
+            for (int r = 0; r < parts; ++r) v += *cluster.map_shared_rank(&part[i], r);
+            const int sc = i >> 1, s = sc / NCH, c = sc % NCH;
+            if (s0 + s < nsk)
+                coef[(((long long)k * ncoef + atom * NCH + c) * ldc + s0 + s) * 2 + (i & 1)] =
+                    ch_scale[atom * NCH + c] * v;
+        }
+    }
+    cluster.sync();  // the other parts keep their shared memory until block 0 has read it
 }
 
 // Complex nonlocal scatter, one thread per grid point: Hu[s][g] += sum_e sum_ch conj(P_e,ch) c[a_e, ch][s],
@@ -258,36 +278,40 @@ __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<double> a) {
 }
 
 template <int NCH>
-void launch_project_z_nch(const DevProjectors& pj, int nk, int nsk, const double* X, long long ldx, long long ldk,
-                          long long xim, double* coef, int forced_sb, cudaStream_t st) {
+int launch_project_z_nch(const DevProjectors& pj, int nk, int nsk, const double* X, long long ldx, long long ldk,
+                         long long xim, double* coef, int forced_sb, int forced_parts, cudaStream_t st) {
     // states per block: the largest of 4 / 2 / 1 (within the register budget of NCH
     // channels) that still gives one block per SM
     constexpr int kMaxSb = NCH <= 4 ? 4 : (NCH == 8 ? 2 : 1);
     const long long zstride = 2LL * pj.nch * pj.npts;
     const long long ldc = coef_ld(nsk);
+    const int parts = project_parts(pj, forced_parts);
     int sb = 1;
     if (forced_sb > 0) {
         sb = std::min(forced_sb, kMaxSb);
     } else {
         for (int c : {4, 2})
-            if (c <= kMaxSb && (long long)pj.na * nk * ((nsk + c - 1) / c) >= 148) {
+            if (c <= kMaxSb && (long long)pj.na * parts * nk * ((nsk + c - 1) / c) >= 148) {
                 sb = c;
                 break;
             }
     }
     const int groups = (nsk + sb - 1) / sb;
-    const dim3 g(pj.na, nk * groups);
+    const dim3 g(pj.na * parts, nk * groups);
+    cudaError_t e;
+#define QG_PROJECT_Z(SBV)                                                                                         \
+    e = launch_clustered(k_project_z<SBV, NCH>, g, dim3(256), parts, st, X, ldx, ldk, xim, nsk, groups,          \
+                         pj.atom_off, pj.pt_g, pj.ztab, zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc, parts)
     if (sb == 4) {
-        if constexpr (kMaxSb >= 4)
-            k_project_z<4, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab,
-                                                   zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
+        if constexpr (kMaxSb >= 4) QG_PROJECT_Z(4);
     } else if (sb == 2) {
-        if constexpr (kMaxSb >= 2)
-            k_project_z<2, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab,
-                                                   zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
-    } else
-        k_project_z<1, NCH><<<g, 256, 0, st>>>(X, ldx, ldk, xim, nsk, groups, pj.atom_off, pj.pt_g, pj.ztab, zstride,
-                                               pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc);
+        if constexpr (kMaxSb >= 2) QG_PROJECT_Z(2);
+    } else {
+        QG_PROJECT_Z(1);
+    }
+#undef QG_PROJECT_Z
+    QG_CUDA_TRY(e);
+    return QG_OK;
 }
 
 template <int NCH>
@@ -389,9 +413,15 @@ int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, co
     if (nonlocal) {
         QG_TRY(ensure_bloch_tables(h, nk, kv, st));
         switch (pj.nch) {
-            case 4: launch_project_z_nch<4>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
-            case 8: launch_project_z_nch<8>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
-            case 16: launch_project_z_nch<16>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, st); break;
+            case 4:
+                QG_TRY(launch_project_z_nch<4>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, h->proj_parts, st));
+                break;
+            case 8:
+                QG_TRY(launch_project_z_nch<8>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, h->proj_parts, st));
+                break;
+            case 16:
+                QG_TRY(launch_project_z_nch<16>(pj, nk, nsk, X, ldx, ldk, N, coef, h->proj_sb, h->proj_parts, st));
+                break;
             default: return QG_ERR_UNSUPPORTED;
         }
     }

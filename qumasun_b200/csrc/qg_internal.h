@@ -1,6 +1,7 @@
 // Internal declarations shared by the engine's translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
@@ -69,6 +70,7 @@ struct DevBuf {
 struct DevProjectors {
     int na = 0, nch = 0;
     long long npts = 0, nent = 0;
+    long long max_atom_pts = 0;  // sphere points of the largest atom
     int* atom_off = nullptr;
     int* pt_g = nullptr;
     double* tab_d = nullptr;
@@ -113,6 +115,7 @@ struct qg_hamiltonian_s {
     int ty = 1;       // grid rows per stencil tile
     int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
     int proj_sb = 0;     // states per projection block (0: chosen per launch)
+    int proj_parts = 0;  // blocks (one cluster) per atom in the projection (0: from the cell)
     int scatter_sg = 0;  // states per scatter group (0: 8)
     qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
     qg_learned learned = nullptr;           // network of precond = 2 (qg_hamiltonian_set_learned)
@@ -159,6 +162,39 @@ struct PhaseTimer {
 constexpr int kHostChunks = 8;
 int host_pipelined_apply(qg_hamiltonian h, int ns, long long row, const double* X, double* HX,
                          const std::function<int(int, const double*, double*)>& apply);
+
+// Launch with `cluster_x` blocks per thread-block cluster along x (1: no cluster).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 block, int cluster_x, cudaStream_t st,
+                                    Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster_x;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = cluster_x > 1 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+// Blocks per atom of the projection (or the forced value), from the cell alone so that
+// results never depend on the batch: one per kProjPartPoints sphere points of the
+// largest atom, doubled for cells of at most 16 atoms (which are solved with few
+// states, so the projection has few blocks and each block's serial walk over its
+// points sets the time), at most 8 (the portable cluster size). Measured on 8-, 64-
+// and 216-atom diamond cells at 16-256 real and 16-128 complex states.
+constexpr int kProjPartPoints = 8192;
+inline int project_parts(const DevProjectors& pj, int forced) {
+    if (forced > 0) return forced;
+    long long p = std::max<long long>(1, (pj.max_atom_pts + kProjPartPoints - 1) / kProjPartPoints);
+    if (pj.na <= 16) p *= 2;
+    return (int)std::min<long long>(8, p);
+}
 
 // Row length of the channel-major projector coefficients [na * nch][ld]: the state
 // count rounded up to 16, so every row starts 128-byte aligned and the scatter's

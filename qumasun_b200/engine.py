@@ -115,7 +115,7 @@ def lib():
                                                    C.POINTER(C.c_float)]
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_set_stencil_kernel.argtypes = [vp, C.c_int]
-        L.qg_hamiltonian_set_nonlocal_blocking.argtypes = [vp, C.c_int, C.c_int]
+        L.qg_hamiltonian_set_nonlocal_blocking.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.qg_context_take_device_status.argtypes = [vp]
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
@@ -486,9 +486,10 @@ class Hamiltonian:
         """False: TMA-staged ring kernel where the shape allows (default); True: register-window kernel."""
         check(lib().qg_hamiltonian_set_stencil_kernel(self.h, 1 if plain else 0), "qg_hamiltonian_set_stencil_kernel")
 
-    def set_nonlocal_blocking(self, project_states=0, scatter_states=0):
-        """States per projection block (1/2/4/8/16) and per scatter group (4/8); 0 = engine's choice."""
-        check(lib().qg_hamiltonian_set_nonlocal_blocking(self.h, project_states, scatter_states),
+    def set_nonlocal_blocking(self, project_states=0, scatter_states=0, project_parts=0):
+        """States per projection block (1/2/4/8/16), per scatter group (4/8) and blocks per
+        atom in the projection (1-8); 0 = engine's choice."""
+        check(lib().qg_hamiltonian_set_nonlocal_blocking(self.h, project_states, scatter_states, project_parts),
               "qg_hamiltonian_set_nonlocal_blocking")
 
     def launches_per_apply(self, ns):

@@ -53,35 +53,53 @@ def test_fp64_and_fp32_match_oracle_diamond8(cuda_ctx, order):
 @pytest.mark.parametrize("kw", [dict(), dict(grid=(12, 12, 12), a0=4.4)], ids=["diamond8", "wrap"])
 def test_nonlocal_blocking_gives_identical_results(cuda_ctx, kw):
     """Every projection / scatter state blocking (and the register-window kernel,
-    which reads the same channel-major coefficients) gives the same bits; the wrap
-    cell has points inside up to 10 projector spheres, past the scatter's register
-    cache of 4 entries."""
+    which reads the same channel-major coefficients) gives the same bits for a given
+    split of each atom's points over a thread-block cluster; every split (1-8 blocks
+    per atom) matches the oracle. The wrap cell has points inside up to 10 projector
+    spheres, past the scatter's register cache of entries."""
     import torch
     from qumasun_b200 import Hamiltonian
     cell = build_cell(**kw)
     X = initial_states(21, cell.N, seed=17)  # ragged against every state group
+    ref = O.hamiltonian_apply(cell, X)
     H = Hamiltonian(cuda_ctx, cell)
     for dt in (torch.float64, torch.float32):
         Xd = torch.from_numpy(X).to("cuda", dt)
-        H.set_nonlocal_blocking(0, 0)
-        base = H.apply(Xd).cpu().numpy()
-        for sb in (1, 2, 4, 8, 16):
-            for sg in (4, 8):
-                H.set_nonlocal_blocking(sb, sg)
-                np.testing.assert_array_equal(H.apply(Xd).cpu().numpy(), base)
-        H.set_nonlocal_blocking(0, 0)
-        H.set_stencil_kernel(True)
-        plain = H.apply(Xd).cpu().numpy()
-        H.set_stencil_kernel(False)
-        ref = O.hamiltonian_apply(cell, X)
         tol = TOL64 if dt == torch.float64 else TOL32
-        assert rel_per_state(base, ref).max() < tol
-        assert rel_per_state(plain, ref).max() < tol
-    with pytest.raises(Exception):
-        H.set_nonlocal_blocking(3, 0)
-    with pytest.raises(Exception):
-        H.set_nonlocal_blocking(0, 16)
+        for parts in (1, 3, 8):
+            H.set_nonlocal_blocking(0, 0, parts)
+            base = H.apply(Xd).cpu().numpy()
+            assert rel_per_state(base, ref).max() < tol
+            for sb in (1, 2, 4, 8, 16):
+                for sg in (4, 8):
+                    H.set_nonlocal_blocking(sb, sg, parts)
+                    np.testing.assert_array_equal(H.apply(Xd).cpu().numpy(), base)
+            H.set_nonlocal_blocking(0, 0, parts)
+            H.set_stencil_kernel(True)
+            plain = H.apply(Xd).cpu().numpy()
+            H.set_stencil_kernel(False)
+            assert rel_per_state(plain, ref).max() < tol
+        H.set_nonlocal_blocking(0, 0, 0)
+    for bad in ((3, 0, 0), (0, 16, 0), (0, 0, 9), (0, 0, -1)):
+        with pytest.raises(Exception):
+            H.set_nonlocal_blocking(*bad)
     H.close()
+
+
+def test_projection_split_does_not_depend_on_the_batch(cuda_ctx):
+    """The engine's split of the projection depends on the cell only: a state gives
+    the same bits applied alone, in a batch of 5 and in a batch of 40."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell()
+    X = torch.from_numpy(initial_states(40, cell.N, seed=23)).cuda()
+    H = Hamiltonian(cuda_ctx, cell)
+    full = H.apply(X).cpu().numpy()
+    five = H.apply(X[:5].contiguous()).cpu().numpy()
+    one = H.apply(X[:1].contiguous()).cpu().numpy()
+    H.close()
+    np.testing.assert_array_equal(five, full[:5])
+    np.testing.assert_array_equal(one, full[:1])
 
 
 def test_displaced_cell_no_nonlocal_and_no_potential(cuda_ctx):
