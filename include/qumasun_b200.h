@@ -174,8 +174,9 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian ham, int ns, const double* X, lo
  * touch the allocator, hosts whose device memory belongs to another framework.
  * It allocates nothing: the projector coefficients go to a scratch array
  * compiled into the library, qg_noalloc_scratch_capacity() doubles (4 MiB) per
- * device, which must hold ns * n_atoms * n_channels values (n_channels = 4 for
- * s+p projectors); larger batches return QG_ERR_UNSUPPORTED. The first call on
+ * device, which must hold ns16 * n_atoms * n_channels values (ns16 = ns rounded
+ * up to a multiple of 16; n_channels = 4 for s+p projectors); larger batches
+ * return QG_ERR_UNSUPPORTED. The first call on
  * a device looks up the array's device address (a CUDA runtime query, no
  * allocation), so make that first call before any stream capture. All calls
  * on a device share the array and it keeps the last call's contents (each call
