@@ -319,6 +319,13 @@ int qg_hamiltonian_set_learned(qg_hamiltonian ham, qg_learned nn, double vscale)
  * for the stream when info is given. */
 int qg_sygv_small_batched_d(qg_context ctx, int batch, int k, const double* A, const double* B, int lda,
                             long long stride, double* w, double* Z, int* info);
+/* Complex Hermitian counterpart: A, B, Z hold interleaved {re, im} doubles (k x k
+ * complex, column-major, leading dimension lda complex elements, stride in complex
+ * elements, lower triangles read); Z + b*k*k (ld k). Replaces lapack_ZHEGVX
+ * (w_zhegvx.h:24-107: ITYPE 1, JOBZ V, RANGE A) for k <= 56, the pencils of the
+ * k-point LOBPCG with up to 18 states per k-point. info as above. */
+int qg_hegv_small_batched_z(qg_context ctx, int batch, int k, const double* A, const double* B, int lda,
+                            long long stride, double* w, double* Z, int* info);
 
 /* Selects the stencil kernel of an operator: 0 = the TMA-staged ring kernel
  * where the shape and alignment allow (default), 1 = always the

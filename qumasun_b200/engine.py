@@ -120,6 +120,7 @@ def lib():
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
+        L.qg_hegv_small_batched_z.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp, C.c_int]
         L.qg_learned_create.argtypes = [vp, C.POINTER(vp)]
@@ -207,6 +208,23 @@ def sygv_small_batched(ctx, A, B):
     check(lib().qg_sygv_small_batched_d(ctx.h, bsz, k, C.c_void_p(At.data_ptr()), C.c_void_p(Bt.data_ptr()), k,
                                         k * k, C.c_void_p(w.data_ptr()), C.c_void_p(Z.data_ptr()),
                                         info.ctypes.data_as(_ip)), "qg_sygv_small_batched_d")
+    return w, Z.transpose(1, 2), info
+
+
+def hegv_small_batched(ctx, A, B):
+    """Batched Hermitian A z = lambda B z for torch CUDA complex128 tensors (batch, k, k)
+    (lower triangles read). Returns (w (batch, k), Z (batch, k, k) columns = eigenvectors, info)."""
+    import torch
+    bsz, k, _ = A.shape
+    At = A.transpose(1, 2).contiguous()   # column-major per problem
+    Bt = B.transpose(1, 2).contiguous()
+    w = torch.empty(bsz, k, dtype=torch.float64, device=A.device)
+    Z = torch.empty(bsz, k, k, dtype=torch.complex128, device=A.device)
+    info = np.zeros(bsz, dtype=np.int32)
+    ctx.use_torch_stream()
+    check(lib().qg_hegv_small_batched_z(ctx.h, bsz, k, C.c_void_p(At.data_ptr()), C.c_void_p(Bt.data_ptr()), k,
+                                        k * k, C.c_void_p(w.data_ptr()), C.c_void_p(Z.data_ptr()),
+                                        info.ctypes.data_as(_ip)), "qg_hegv_small_batched_z")
     return w, Z.transpose(1, 2), info
 
 
