@@ -156,7 +156,10 @@ struct WorkGrid {
 // the real and the imaginary rows of one plane, and each point adds the
 // first-derivative coupling -(1/2) 2i g.grad between the two parts
 // (LaplasianKpoint8th_halo_f, GridDifferenceKpoint8th.h:18-122).
-template <typename T, int ORDER, int PX, int NC>
+// NXC > 0: the row length nx as a compile-time constant (instantiated for the common
+// grids), so that the y-neighbour offsets +-d*nx become immediate offsets of the
+// shared-memory loads instead of per-load address arithmetic.
+template <typename T, int ORDER, int PX, int NC, int NXC>
 __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
     k_stencil_tma(const HamArgs<T> a, const WorkGrid wg, int nst) {
     constexpr int R = radius<ORDER>();
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
     volatile int* ctl = reinterpret_cast<volatile int*>(empty + nst);  // [0] abort, [1] last position issued
     T* ring = reinterpret_cast<T*>(smem + kBarBytes);
 
-    const int nx = a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
+    const int nx = NXC > 0 ? NXC : a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
     const int rows = ty + 2 * R;
     const int comp_elems = rows * nx;  // one part (real or imaginary) of a plane
     const int stage_elems = NC * comp_elems;
@@ -448,15 +451,25 @@ int sm_count() {
     return n;
 }
 
-template <typename T, int ORDER, int NC>
+template <typename T, int ORDER, int NC, int NXC = 0>
 int launch_order(const HamArgs<T>& a, cudaStream_t st) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = radius<ORDER>();
+    if constexpr (NXC == 0 && ORDER == 8 && sizeof(T) == 8) {
+        // FP64 order 8 (the reference's default): row lengths of the common grids
+        // compiled in
+        switch (a.nx) {
+            case 40: return launch_order<T, ORDER, NC, 40>(a, st);
+            case 80: return launch_order<T, ORDER, NC, 80>(a, st);
+            case 120: return launch_order<T, ORDER, NC, 120>(a, st);
+            default: break;
+        }
+    }
     const size_t stage = (size_t)NC * (a.ty + 2 * R) * a.nx * sizeof(T);
     const int nst = ring_stages_for(R, stage);
     if (nst < 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = kBarBytes + (size_t)nst * stage;
-    auto kern = k_stencil_tma<T, ORDER, PX, NC>;
+    auto kern = k_stencil_tma<T, ORDER, PX, NC, NXC>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * a.ty;
