@@ -404,6 +404,11 @@ __global__ void __launch_bounds__(256, SG <= 4 ? 3 : 2) k_scatter_all(T* __restr
         }
     }
     for (int s0 = 0; s0 < ns; s0 += SG) {
+        // the group's H psi values load first, so their latency overlaps the sums
+        const int gn = min(SG, ns - s0);
+        T h[SG];
+#pragma unroll
+        for (int s = 0; s < SG; ++s) h[s] = (s < gn) ? HX[(long long)(s0 + s) * ldhx + g] : T(0);
         T acc[SG];
 #pragma unroll
         for (int s = 0; s < SG; ++s) acc[s] = T(0);
@@ -436,10 +441,6 @@ __global__ void __launch_bounds__(256, SG <= 4 ? 3 : 2) k_scatter_all(T* __restr
                 }
             }
         }
-        const int gn = min(SG, ns - s0);
-        T h[SG];
-#pragma unroll
-        for (int s = 0; s < SG; ++s) h[s] = (s < gn) ? HX[(long long)(s0 + s) * ldhx + g] : T(0);
 #pragma unroll
         for (int s = 0; s < SG; ++s)
             if (s < gn) HX[(long long)(s0 + s) * ldhx + g] = h[s] + acc[s];
