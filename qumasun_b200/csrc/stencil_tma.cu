@@ -133,10 +133,10 @@ __device__ __forceinline__ T der_point(const T* xm, const T* xp, const T* ym, co
 }
 
 constexpr int kBarBytes = 1024;  // mbarriers + control words at the front of dynamic shared memory
-constexpr int kMaxThreads = 416;
-constexpr int kMaxConsumers = 384;
-constexpr int kMaxThreadsKp = 288;  // complex states keep two register windows per thread
-constexpr int kMaxConsumersKp = 256;
+constexpr int kMaxThreads = 448;
+constexpr int kMaxConsumers = 416;
+constexpr int kMaxThreadsKp = 352;  // complex states keep two register windows per thread
+constexpr int kMaxConsumersKp = 320;
 constexpr int kMaxStages = 16;
 
 template <int ORDER>
@@ -423,9 +423,10 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
 
 // Rows per tile: the largest divisor of ny (<= 16) keeping the consumer threads within the kernel's limit.
 template <typename T>
-int tma_tile_rows(const HamArgs<T>& a, int nc) {
+int tma_tile_rows(const HamArgs<T>& a, int nc, int order) {
     constexpr int PX = 16 / sizeof(T);
-    const int maxc = nc == 1 ? kMaxConsumers : kMaxConsumersKp;
+    // order 2 (3-plane window, DRAM-bound) measured fastest with at most 384 consumers
+    const int maxc = nc == 1 ? (order == 2 ? 384 : kMaxConsumers) : kMaxConsumersKp;
     int ty = 0;
     for (int t = 1; t <= 16; ++t)
         if (a.ny % t == 0 && (a.nx / PX) * t <= maxc) ty = t;
@@ -505,7 +506,7 @@ bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc) {
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R)
         return false;
-    const int ty = tma_tile_rows(a, nc);
+    const int ty = tma_tile_rows(a, nc, order);
     if (ty == 0) return false;
     const size_t stage = (size_t)nc * (ty + 2 * R) * a.nx * sizeof(T);
     return ring_stages_for(R, stage) > 0;
@@ -517,7 +518,7 @@ template <typename T>
 int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc) {
     if (!stencil_tma_ok<T>(a, order, nc)) return QG_ERR_UNSUPPORTED;
     HamArgs<T> b = a;
-    b.ty = tma_tile_rows(a, nc);
+    b.ty = tma_tile_rows(a, nc, order);
     if (nc == 2) {
         if constexpr (sizeof(T) == 8) return launch_order<T, 8, 2>(b, st);
         return QG_ERR_UNSUPPORTED;
