@@ -34,8 +34,8 @@ NS = 256
 REPS = (2, 2, 2)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_stencil_tma launch per
 # state of this workload, from an ncu --set full capture of the same bench at 32 states
-# (234.6 MB / 32); traffic grows in proportion to the states, so a full launch is scaled.
-STENCIL_DRAM_BYTES_PER_STATE = 234604544 / 32
+# (229.9 MB / 32); traffic grows in proportion to the states, so a full launch is scaled.
+STENCIL_DRAM_BYTES_PER_STATE = 229949440 / 32
 FD_ORDER = 8
 WORKLOAD = "diamond64_80cube_Hpsi"
 

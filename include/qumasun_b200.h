@@ -334,8 +334,8 @@ int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int plain);
 /* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
  * complex states use at most 4), states per scatter group of the real apply (4 or
  * 8), and blocks per atom in the projection (1-8, one thread-block cluster; the
- * engine's choice follows the cell alone: one per 8192 sphere points, doubled for
- * cells of at most 16 atoms); 0 = the
+ * engine's choice follows the cell alone: 1 for cells of more than 16 atoms, else
+ * one per 4096 sphere points of the largest atom); 0 = the
  * engine's choice. The block sizes do not change the result (same sums in the same
  * order); the parts per atom change the summation order of the projections (last
  * bits only), and the engine's choice never depends on the number of states. */

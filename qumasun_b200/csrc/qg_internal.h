@@ -183,16 +183,18 @@ inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 bloc
 }
 
 // Blocks per atom of the projection (or the forced value), from the cell alone so that
-// results never depend on the batch: one per kProjPartPoints sphere points of the
-// largest atom, doubled for cells of at most 16 atoms (which are solved with few
-// states, so the projection has few blocks and each block's serial walk over its
-// points sets the time), at most 8 (the portable cluster size). Measured on 8-, 64-
-// and 216-atom diamond cells at 16-256 real and 16-128 complex states.
-constexpr int kProjPartPoints = 8192;
+// results never depend on the batch: one block per atom for cells of more than 16
+// atoms (enough blocks already), and for smaller cells (solved with few states, where
+// each block's serial walk over its points sets the time) one per kProjPartPoints
+// sphere points of the largest atom, at most 8 (the portable cluster size). Measured on
+// 8-, 64- and 216-atom diamond cells at 16-256 real and 16-128 complex states; on the
+// large cells 2 parts were within 2 % of 1 and changed the last bits of H enough to
+// take the 216-atom LOBPCG (480 of 528 states) from 40 to 102 iterations.
+constexpr int kProjPartPoints = 4096;
 inline int project_parts(const DevProjectors& pj, int forced) {
     if (forced > 0) return forced;
-    long long p = std::max<long long>(1, (pj.max_atom_pts + kProjPartPoints - 1) / kProjPartPoints);
-    if (pj.na <= 16) p *= 2;
+    if (pj.na > 16) return 1;
+    const long long p = std::max<long long>(1, (pj.max_atom_pts + kProjPartPoints - 1) / kProjPartPoints);
     return (int)std::min<long long>(8, p);
 }
 
