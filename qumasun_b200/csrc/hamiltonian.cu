@@ -205,8 +205,31 @@ __global__ void __launch_bounds__(1024) k_hamiltonian(const HamArgs<T> a) {
 // together, so their overlapping spheres are gathered from L2.
 // The coefficients are stored channel-major, coef[(atom * NCH + ch) * ldc + s], so
 // that the scatter reads the states of one (atom, channel) as contiguous vectors.
-template <typename T, int SB, int NCH>
-__global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long long ldx, int ns,
+__device__ __forceinline__ uint32_t smem_u32addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Asynchronous gather of one element into shared memory (no register holds it in flight).
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32addr(smem)), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr int kProjThreads = 256;
+// DEPTH > 0: the states at a point and its table values are gathered with cp.async into
+// a DEPTH-stage ring of per-thread shared-memory slots (each thread reads back only its
+// own slots, so no block barrier), the grid indices DEPTH points ahead in registers:
+// DEPTH - 1 points' gathers stay in flight without holding registers. The points of a
+// thread and the order of its sums are those of the register path (DEPTH = 0), so the
+// result is the same to the bit.
+template <typename T, int SB, int NCH, int DEPTH>
+__global__ void __launch_bounds__(kProjThreads) k_project(const T* __restrict__ X, long long ldx, int ns,
                                                  const int* __restrict__ atom_off,
                                                  const int* __restrict__ pt_g,
                                                  const T* __restrict__ tab, long long npts,
@@ -228,6 +251,58 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
 #pragma unroll
     for (int s = 0; s < SB; ++s) Xs[s] = X + (long long)min(s0 + s, ns - 1) * ldx;
 
+    if constexpr (DEPTH > 0) {
+        extern __shared__ __align__(16) unsigned char proj_dsm[];
+        T* ring = reinterpret_cast<T*>(proj_dsm);  // [DEPTH][SB + NCH][kProjThreads]
+        const int tid = threadIdx.x;
+        auto slot = [&](int d, int q) { return ring + ((size_t)d * (SB + NCH) + q) * kProjThreads + tid; };
+        auto issue = [&](int d, int g, int pt) {
+#pragma unroll
+            for (int s = 0; s < SB; ++s) cp_async_elem(slot(d, s), Xs[s] + g);
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) cp_async_elem(slot(d, SB + c), tab + (long long)c * npts + pt);
+        };
+        const int niter = (p1 - p0 + kProjThreads - 1) / kProjThreads;  // the same for the whole block
+#pragma unroll
+        for (int j = 0; j < DEPTH - 1; ++j) {
+            const int pj = p0 + tid + j * kProjThreads;
+            if (pj < p1) issue(j, pt_g[pj], pj);
+            cp_async_commit();
+        }
+        int gq[DEPTH];
+#pragma unroll
+        for (int j = DEPTH - 1; j < 2 * DEPTH - 1; ++j) {
+            const int pj = p0 + tid + j * kProjThreads;
+            gq[j % DEPTH] = pj < p1 ? pt_g[pj] : 0;
+        }
+        for (int i0 = 0; i0 < niter; i0 += DEPTH) {
+#pragma unroll
+            for (int u = 0; u < DEPTH; ++u) {
+                const int i = i0 + u;
+                if (i < niter) {
+                    const int sj = (u + DEPTH - 1) % DEPTH;  // slot of point i + DEPTH - 1
+                    const int pj = p0 + tid + (i + DEPTH - 1) * kProjThreads;
+                    if (pj < p1) issue(sj, gq[sj], pj);
+                    const int pr = pj + DEPTH * kProjThreads;
+                    gq[sj] = pr < p1 ? pt_g[pr] : 0;
+                    cp_async_commit();
+                    cp_async_wait<DEPTH - 1>();  // this thread's gathers of point i have landed
+                    if (p0 + tid + i * kProjThreads < p1) {
+                        T tv[NCH];
+#pragma unroll
+                        for (int c = 0; c < NCH; ++c) tv[c] = *slot(u, SB + c);
+#pragma unroll
+                        for (int s = 0; s < SB; ++s) {
+                            const T v = *slot(u, s);
+#pragma unroll
+                            for (int c = 0; c < NCH; ++c) acc[s][c] += tv[c] * v;
+                        }
+                    }
+                }
+            }
+        }
+        cp_async_wait<0>();
+    } else {
     // software pipeline: the grid index and table values of the next point are in
     // flight while the states are gathered at the current one, so each step waits
     // for one memory latency instead of two dependent ones
@@ -262,6 +337,7 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ X, long l
         g = gn;
 #pragma unroll
         for (int c = 0; c < NCH; ++c) tv[c] = tn[c];
+    }
     }
     // block reduction: warp shuffles, then one value per warp through shared memory
     __shared__ T red[8][SB * NCH];
@@ -306,6 +382,8 @@ static int pick_project_sb(int blocks_per_group, int ns, int forced) {
     return 1;
 }
 
+constexpr int kProjDepth = 3;  // cp.async stages of the projection's gather
+
 template <typename T, int NCH>
 static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X, long long ldx, T* coef,
                               long long ldc, int sb, int parts, cudaStream_t st) {
@@ -314,9 +392,15 @@ static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, con
     sb = std::min(sb, kMaxSb);
     const dim3 g(pj.na * parts, (ns + sb - 1) / sb);
     cudaError_t e;
-#define QG_PROJECT(SBV)                                                                                              \
-    e = launch_clustered(k_project<T, SBV, NCH>, g, dim3(256), parts, st, X, ldx, ns, pj.atom_off, pj.pt_g, tab, \
-                         pj.npts, pj.ch_scale, coef, ldc, parts)
+#define QG_PROJECT(SBV)                                                                                        \
+    do {                                                                                                       \
+        const size_t smem = (size_t)kProjDepth * (SBV + NCH) * kProjThreads * sizeof(T);                       \
+        auto kern = k_project<T, SBV, NCH, kProjDepth>;                                                        \
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) \
+            return QG_ERR_CUDA;                                                                                \
+        e = launch_clustered(kern, g, dim3(kProjThreads), parts, smem, st, X, ldx, ns, pj.atom_off, pj.pt_g,   \
+                             tab, pj.npts, pj.ch_scale, coef, ldc, parts);                                     \
+    } while (0)
     switch (sb) {
         case 16:
             if constexpr (kMaxSb >= 16) {

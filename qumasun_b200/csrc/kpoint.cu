@@ -300,7 +300,7 @@ int launch_project_z_nch(const DevProjectors& pj, int nk, int nsk, const double*
     const dim3 g(pj.na * parts, nk * groups);
     cudaError_t e;
 #define QG_PROJECT_Z(SBV)                                                                                         \
-    e = launch_clustered(k_project_z<SBV, NCH>, g, dim3(256), parts, st, X, ldx, ldk, xim, nsk, groups,          \
+    e = launch_clustered(k_project_z<SBV, NCH>, g, dim3(256), parts, 0, st, X, ldx, ldk, xim, nsk, groups,       \
                          pj.atom_off, pj.pt_g, pj.ztab, zstride, pj.npts, pj.ch_scale, coef, pj.na * NCH, ldc, parts)
     if (sb == 4) {
         if constexpr (kMaxSb >= 4) QG_PROJECT_Z(4);

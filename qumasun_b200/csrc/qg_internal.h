@@ -165,12 +165,12 @@ int host_pipelined_apply(qg_hamiltonian h, int ns, long long row, const double* 
 
 // Launch with `cluster_x` blocks per thread-block cluster along x (1: no cluster).
 template <typename... KArgs, typename... Args>
-inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 block, int cluster_x, cudaStream_t st,
-                                    Args... args) {
+inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 block, int cluster_x, size_t smem,
+                                    cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
