@@ -54,9 +54,11 @@ def parse():
     p.add_argument("--states", type=int, default=NS, help="states per apply (smaller for profiling captures)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     p.add_argument("--no-kpoint", action="store_true", help="skip the k-point leg (64 Monkhorst-Pack points)")
+    p.add_argument("--no-cells", action="store_true",
+                   help="skip the 16-cell leg (8- to 64-atom cells solved one by one and together)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-preconditioner leg (GPU training and an unseen-cell comparison)")
-    p.add_argument("--only", choices=["kpoint", "gram"], default=None,
+    p.add_argument("--only", choices=["kpoint", "gram", "cells"], default=None,
                    help="run one leg alone and print its JSON (profiling captures)")
     p.add_argument("--kpoints", type=int, default=64, help="k-points of the k-point leg (4x4x4 grid order)")
     p.add_argument("--gram-rows", type=int, default=1_728_000, help="rows N of the --only gram leg")
@@ -413,6 +415,60 @@ def learned_leg(ctx, steps=1500):
             "lobpcg_unseen_cell": cmp}
 
 
+def cells_leg():
+    """16 cells of uneven size solved together: 4 each of the 8-atom (40^3), 16-atom
+    (80x40x40), 32-atom (80x80x40) and 64-atom (80^3) diamond supercells, atoms displaced
+    by seeded Gaussian sigma 0.05 bohr, 2 states per atom to 1e-10 (plus a 1/8 guard
+    band), kinetic-preconditioned FP64 LOBPCG. Each cell has its own context and stream.
+    Times the 16 solves one after another and all at once (qg_lobpcg_cells_device) and
+    checks that both give the same eigenvalues."""
+    import numpy as np
+    import torch
+    from qumasun_b200 import Context, Hamiltonian
+    from qumasun_b200.cell import build_cell, initial_states
+    from qumasun_b200.engine import lobpcg_cells
+    shapes = [(1, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2)]
+    cells, X0, nconv = [], [], []
+    for i in range(16):
+        reps = shapes[i // 4]
+        cell = build_cell(reps=reps, displacement=0.05, seed=100 + i)
+        nc = 2 * cell.n_atoms
+        cells.append(cell)
+        nconv.append(nc)
+        X0.append(initial_states(nc + nc // 8, cell.N, seed=200 + i))
+    ctxs = [Context(0) for _ in cells]
+    hams = [Hamiltonian(c, cell) for c, cell in zip(ctxs, cells)]
+    # one by one (each cell on its own context, the contexts used in turn)
+    t0 = time.perf_counter()
+    one = []
+    for c in range(16):
+        r = hams[c].lobpcg_device(torch.from_numpy(X0[c]).cuda(), None, max_iter=1000, precond=1,
+                                  n_converge=nconv[c])
+        one.append(r)
+    torch.cuda.synchronize()
+    t_one = time.perf_counter() - t0
+    Xs = [torch.from_numpy(x).cuda() for x in X0]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out, rc = lobpcg_cells(hams, Xs, max_iter=1000, precond=1, n_converge=nconv)
+    torch.cuda.synchronize()
+    t_all = time.perf_counter() - t0
+    diff = max(float(np.abs(out[c]["ev"][:nconv[c]] - one[c]["ev"][:nconv[c]]).max()) for c in range(16))
+    res = {"workload": "16_cells_8to64_atoms_40to80_grids_sigma0.05_2states_per_atom_fd8",
+           "cells": [{"atoms": cells[c].n_atoms, "grid": [cells[c].nx, cells[c].ny, cells[c].nz],
+                      "states": int(X0[c].shape[0]), "converge": nconv[c],
+                      "iterations": out[c]["report"]["iterations"], "converged": bool(out[c]["report"]["converged"])}
+                     for c in range(16)],
+           "seconds_one_by_one": round(t_one, 3), "seconds_together": round(t_all, 3),
+           "speedup_together": round(t_one / t_all, 3), "status": rc,
+           "max_abs_ev_diff_together_vs_one_by_one_Ha": diff}
+    for h in hams:
+        h.close()
+    for c in ctxs:
+        c.close()
+    return res
+
+
 def lobpcg_diamond216(ctx):
     """Time to the 480 lowest eigenpairs (528 solved, a 48-state guard band) of the
     216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
@@ -587,6 +643,9 @@ def run_gpu_arm(a):
     lrn = None
     if rank == 0 and not a.no_learned:
         lrn = learned_leg(ctx)
+    cells_res = None
+    if rank == 0 and not a.no_cells:
+        cells_res = cells_leg()
     lob = None
     lob216 = None
     if rank == 0 and not a.no_lobpcg:
@@ -630,6 +689,8 @@ def run_gpu_arm(a):
             line["kpoint"] = kp
         if lrn:
             line["learned_preconditioner"] = lrn
+        if cells_res:
+            line["cells"] = cells_res
         print(json.dumps(line), flush=True)
     H.close()
     ctx.close()
@@ -684,6 +745,8 @@ def run_only(a):
     ctx.use_torch_stream()
     if a.only == "gram":
         out = gram_leg(ctx, N=a.gram_rows, m=a.gram_cols, steps=a.steps)
+    elif a.only == "cells":
+        out = cells_leg()
     else:
         out = kpoint_leg(ctx, n_k=a.kpoints, steps=a.steps)
     print(json.dumps(out), flush=True)

@@ -265,6 +265,18 @@ int qg_lobpcg_zk_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int nk
 /* Same with DEVICE buffers X and P (ld = 2N); ev stays a host array. */
 int qg_lobpcg_z_device(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev,
                        double* X, double* P, qg_lobpcg_report* report);
+/* Real LOBPCG (qg_lobpcg_d_device) on several independent cells at once: cell c has
+ * operator hams[c], options opts[c], ns[c] states, DEVICE X[c] / P[c] (P may be NULL
+ * when every opts[c].first_call is set), HOST ev[c]; reports[c] and status[c] (either
+ * may be NULL) receive each cell's report and status. Each cell must use its own
+ * context (its stream and library handles); the cells' solves run concurrently on
+ * their streams, so small cells fill the GPU together. Returns QG_OK or the first
+ * failing cell's status. No counterpart in the reference, which solves one cell per
+ * run (EigenLOBPCG_d_multi, lobpcg_d_multi.h:23-27, called per spin by
+ * qumasun_single.lobpcg.h:17-34). */
+int qg_lobpcg_cells_device(int ncells, const qg_hamiltonian* hams, const qg_lobpcg_options* opts, const int* ns,
+                           double* const* ev, double* const* X, double* const* P, qg_lobpcg_report* reports,
+                           int* status);
 
 /* No counterpart in the reference (its Gram products are FP64 BLAS, w_dgemm.h:32-36).
  * C (m x m, column-major, ld m) = alpha * A^T B for DEVICE blocks A, B (N x m,

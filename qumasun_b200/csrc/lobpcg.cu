@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "gram_mixed.h"
@@ -1198,6 +1199,33 @@ int qg_lobpcg_d_device(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, d
                        qg_lobpcg_report* rep) {
     if (!X || (!P && opt && !opt->first_call)) return QG_ERR_INVALID;
     return run_lobpcg(h, opt, ns, 1, ev, X, P, nullptr, nullptr, nullptr, nullptr, rep);
+}
+
+int qg_lobpcg_cells_device(int ncells, const qg_hamiltonian* hams, const qg_lobpcg_options* opts, const int* ns,
+                           double* const* ev, double* const* X, double* const* P, qg_lobpcg_report* reports,
+                           int* status) {
+    if (ncells <= 0 || !hams || !opts || !ns || !ev || !X) return QG_ERR_INVALID;
+    for (int c = 0; c < ncells; ++c) {
+        if (!hams[c] || !X[c] || !ev[c] || ns[c] <= 0) return QG_ERR_INVALID;
+        if (!opts[c].first_call && (!P || !P[c])) return QG_ERR_INVALID;
+        for (int d = 0; d < c; ++d)  // one context (stream and library handles) per cell
+            if (hams[d]->ctx == hams[c]->ctx) return QG_ERR_INVALID;
+    }
+    std::vector<int> st(ncells, QG_OK);
+    std::vector<std::thread> pool;
+    pool.reserve(ncells);
+    for (int c = 0; c < ncells; ++c)
+        pool.emplace_back([&, c] {
+            st[c] = run_lobpcg(hams[c], &opts[c], ns[c], 1, ev[c], X[c], P ? P[c] : nullptr, nullptr, nullptr,
+                               nullptr, nullptr, reports ? &reports[c] : nullptr);
+        });
+    for (auto& t : pool) t.join();
+    int rc = QG_OK;
+    for (int c = 0; c < ncells; ++c) {
+        if (status) status[c] = st[c];
+        if (rc == QG_OK && st[c] != QG_OK) rc = st[c];
+    }
+    return rc;
 }
 
 int qg_lobpcg_z(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,

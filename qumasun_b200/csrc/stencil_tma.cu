@@ -442,13 +442,12 @@ int ring_stages_for(int R, size_t stage_bytes) {
 }
 
 int sm_count() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
+    static const int n = [] {  // initialised once, also when several host threads launch
+        int dev = 0, c = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        return c > 0 ? c : 148;
+    }();
     return n;
 }
 

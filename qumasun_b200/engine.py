@@ -142,6 +142,9 @@ def lib():
                                          C.POINTER(LobpcgReport)]
         L.qg_lobpcg_d_device.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp,
                                          C.POINTER(LobpcgReport)]
+        L.qg_lobpcg_cells_device.argtypes = [C.c_int, C.POINTER(vp), C.POINTER(LobpcgOptions), _ip,
+                                             C.POINTER(_dp), C.POINTER(vp), C.POINTER(vp),
+                                             C.POINTER(LobpcgReport), _ip]
         _lib = L
     return _lib
 
@@ -209,6 +212,45 @@ def sygv_small_batched(ctx, A, B):
                                         k * k, C.c_void_p(w.data_ptr()), C.c_void_p(Z.data_ptr()),
                                         info.ctypes.data_as(_ip)), "qg_sygv_small_batched_d")
     return w, Z.transpose(1, 2), info
+
+
+def lobpcg_cells(hams, Xs, Ps=None, max_iter=2000, tol=1.0e-10, first=True, precond=1, shift=1.0,
+                 n_converge=None, precision=0):
+    """Real LOBPCG on several independent cells at once (qg_lobpcg_cells_device).
+
+    hams: Hamiltonians, each on its own Context; Xs: float64 CUDA tensors (ns_c, N_c),
+    overwritten with the eigenvectors; Ps: matching tensors (or None on a first call);
+    n_converge: per-cell counts of states that must converge (None: all). Each cell's
+    context is put on its own CUDA stream so that the solves overlap on the GPU.
+    Returns (list of dict(ev, report, status), overall status)."""
+    import torch
+    n = len(hams)
+    assert n == len(Xs) and len({id(h.ctx) for h in hams}) == n, "one context per cell"
+    for X in Xs:
+        assert X.is_cuda and X.dtype == torch.float64 and X.is_contiguous()
+    streams = [torch.cuda.Stream(device=X.device) for X in Xs]
+    torch.cuda.synchronize()  # inputs written on other streams are complete
+    for h, s in zip(hams, streams):
+        h.ctx.set_stream(s.cuda_stream)
+        h.ctx.cells_stream = s  # keeps the stream alive while the context may use it
+    ncs = [0] * n if n_converge is None else list(n_converge)
+    opts = (LobpcgOptions * n)(*[LobpcgOptions(max_iter, tol, 1 if first else 0, precision, 0, precond, shift,
+                                               ncs[c]) for c in range(n)])
+    reps = (LobpcgReport * n)()
+    ns = np.array([X.shape[0] for X in Xs], dtype=np.int32)
+    evs = [np.zeros(int(k)) for k in ns]
+    ev_ptrs = (_dp * n)(*[e.ctypes.data_as(_dp) for e in evs])
+    x_ptrs = (C.c_void_p * n)(*[X.data_ptr() for X in Xs])
+    p_ptrs = (C.c_void_p * n)(*[(P.data_ptr() if P is not None else 0) for P in (Ps or [None] * n)])
+    h_ptrs = (C.c_void_p * n)(*[h.h.value if isinstance(h.h, C.c_void_p) else h.h for h in hams])
+    status = np.zeros(n, dtype=np.int32)
+    rc = lib().qg_lobpcg_cells_device(n, h_ptrs, opts, ns.ctypes.data_as(_ip), ev_ptrs, x_ptrs, p_ptrs, reps,
+                                      status.ctypes.data_as(_ip))
+    for st in status:
+        if st not in (QG_OK, -9):
+            check(int(st), "qg_lobpcg_cells_device")
+    out = [dict(ev=evs[c], report=reps[c].as_dict(), status=int(status[c])) for c in range(n)]
+    return out, rc
 
 
 def hegv_small_batched(ctx, A, B):

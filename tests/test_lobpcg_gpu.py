@@ -91,3 +91,35 @@ def test_mixed_precision_gram_reaches_fp64_eigenvalues(cuda_ctx):
     H.close()
     assert r["status"] == 0 and r["report"]["converged"] == 1
     np.testing.assert_allclose(np.sort(r["ev"]), np.sort(g["ev"]), rtol=0, atol=1e-8)
+
+
+def test_cells_solved_together_match_one_by_one(cuda_ctx):
+    """qg_lobpcg_cells_device: three cells of different grids (the 8-atom 40^3 cell of
+    the reference fixture, a displaced 16-atom 80x40x40 cell and a small 24x20x16 cell),
+    each on its own context and stream, solved concurrently, give the eigenvalues of
+    solving them one by one, and the 8-atom cell the reference solver's."""
+    import torch
+    from qumasun_b200 import Context, Hamiltonian
+    from qumasun_b200.engine import lobpcg_cells
+    g = np.load(os.path.join(GOLD, "lobpcg_diamond8.npz"))
+    cells = [build_cell(), build_cell(reps=(2, 1, 1), displacement=0.05, seed=7), build_cell(grid=(24, 20, 16))]
+    ns = [int(g["ns"]), 34, 6]
+    nconv = [int(g["ns"]), 32, 6]
+    X0 = [initial_states(ns[0], cells[0].N, seed=int(g["seed"])), initial_states(ns[1], cells[1].N, seed=8),
+          initial_states(ns[2], cells[2].N, seed=9)]
+    ctxs = [Context(0) for _ in cells]
+    hams = [Hamiltonian(c, cell) for c, cell in zip(ctxs, cells)]
+    Xs = [torch.from_numpy(x).cuda() for x in X0]
+    out, rc = lobpcg_cells(hams, Xs, max_iter=3000, precond=1, n_converge=nconv)
+    assert rc == 0 and all(o["status"] == 0 and o["report"]["converged"] == 1 for o in out)
+    for c in range(3):
+        one = hams[c].lobpcg_device(torch.from_numpy(X0[c]).cuda(), None, max_iter=3000, precond=1,
+                                    n_converge=nconv[c])
+        np.testing.assert_allclose(out[c]["ev"][:nconv[c]], one["ev"][:nconv[c]], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(np.sort(out[0]["ev"]), g["ev"], rtol=0, atol=EV_TOL)
+    with pytest.raises(AssertionError):
+        lobpcg_cells([hams[0], hams[0]], [Xs[0], Xs[0]])  # one context per cell
+    for h in hams:
+        h.close()
+    for c in ctxs:
+        c.close()
