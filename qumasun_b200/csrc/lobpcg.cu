@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "gram_mixed.h"
+#include "gram_ts.h"
 #include "precond.h"
 #include "qg_internal.h"
 #include "small_eig.h"
@@ -350,6 +351,7 @@ struct Solver {
     cublasHandle_t blas;
     cusolverDnHandle_t sol;
     DevBuf W, AW, T, S, E, small, work, heg;  // heg: batched complex pencils (k-point solve)
+    DevBuf gts;                                // partial sums of the tall-skinny Gram kernel
     int lwork = 0;
     double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *Sa, *Sb, *Sa2, *Sb2, *M;
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
@@ -363,7 +365,7 @@ struct Solver {
 
     ~Solver() {
         W.release(); AW.release(); T.release(); S.release(); E.release(); small.release();
-        work.release(); heg.release();
+        work.release(); heg.release(); gts.release();
     }
 
     int setup() {
@@ -459,6 +461,12 @@ struct Solver {
             QG_TRY(mg.gram(blas, st, m, false, c == 1, dV, Sa, m, h->ctx->dev_status));
             QG_TRY(mg.gram(blas, st, m, true, c == 1, dV, Sb, m, h->ctx->dev_status));
             return QG_OK;
+        }
+        if (c == 1 && m <= qg::kGramTsUpTo) {
+            // small real pencils: K split over the GPU (cuBLAS's DSYRK took 3.5 ms per
+            // iteration at 48 columns x 64k rows; complex pencils measured faster on cuBLAS)
+            QG_TRY(gts.reserve(qg::gram_ts_scratch_doubles(N, 1, true) * sizeof(double)));
+            return qg::gram_ts_tiled(x, N, 0, Ax, x, N, 0, N, m, m, dV, Sa, Sb, m, 0, 1, gts.as<double>(), st);
         }
         if (c == 2) {
             QG_TRY(gemm_tn(m, m, x, Ax, dV, Sa, m));
@@ -954,6 +962,11 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
                                     (int)N, B + k * kstride, (int)N, &zero, C + k * gsz, g));
         return QG_OK;
     };
+    auto gram_pair = [&](const double* Wi, const double* AWj, const double* Wj, double* Ca_, double* Cb_,
+                         int g) -> int {
+        QG_TRY(gram_block(Wi, AWj, Ca_, g));
+        return gram_block(Wi, Wj, Cb_, g);
+    };
     // C_k (N x 2nb) = A_k (N x 2nb) * Z_k (rows off.., ldz) + beta C_k, batched over k
     auto rot_block = [&](const double* A, const double* Z, int ldz, double* C, double beta) -> int {
         const double one = 1.0;
@@ -1007,8 +1020,7 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         for (int bi = 0; bi < k3 / nb; ++bi)
             for (int bj = 0; bj <= bi; ++bj) {
                 const size_t off = (size_t)bi * 2 * nb + (size_t)bj * 2 * nb * g;
-                QG_TRY(gram_block(Wb[bi], AWb[bj], SaAll + off, g));
-                QG_TRY(gram_block(Wb[bi], Wb[bj], SbAll + off, g));
+                QG_TRY(gram_pair(Wb[bi], AWb[bj], Wb[bj], SaAll + off, SbAll + off, g));
             }
         // Hermitian pencils k by k; solutions expanded to real rotations M_k (2k3 x 2nb)
         tm.mark(2, st);
