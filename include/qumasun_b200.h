@@ -153,6 +153,12 @@ int qg_hamiltonian_apply_z(qg_hamiltonian ham, int ns, const double* X, long lon
  * the reference, which loops over k (qumasun_kpoint.lobpcg.h:25-41). */
 int qg_hamiltonian_apply_zk(qg_hamiltonian ham, int nk, const double* kvecs, int nsk, const double* X,
                             long long ldx, long long ldk, double* HX, long long ldhx, long long ldkh);
+/* Complex64 states (FP32 {re[N], im[N]} per state): the same operator with FP32
+ * stencil, potential, Bloch tables and projector sums (the FP32 counterpart of
+ * qg_hamiltonian_apply_f for k-points); single k-vector / several k-points. */
+int qg_hamiltonian_apply_zf(qg_hamiltonian ham, int ns, const float* X, long long ldx, float* HX, long long ldhx);
+int qg_hamiltonian_apply_zkf(qg_hamiltonian ham, int nk, const double* kvecs, int nsk, const float* X,
+                             long long ldx, long long ldk, float* HX, long long ldhx, long long ldkh);
 /* qg_hamiltonian_apply_z with HOST buffers (ns * 2N doubles each, ldx = 2N). */
 int qg_hamiltonian_apply_host_z(qg_hamiltonian ham, int ns, const double* X, double* HX);
 /* qg_hamiltonian_apply_z with the phase timing of qg_hamiltonian_apply_timed_d. */

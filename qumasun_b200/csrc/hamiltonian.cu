@@ -720,6 +720,7 @@ void free_projectors(DevProjectors& pj) {
     cudaFree(pj.atom_off); cudaFree(pj.pt_g); cudaFree(pj.tab_d); cudaFree(pj.tab_f);
     cudaFree(pj.ch_scale); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
     cudaFree(pj.ent_val_f); cudaFree(pj.pt_u); cudaFree(pj.ent_pt); cudaFree(pj.ztab); cudaFree(pj.zent);
+    cudaFree(pj.ztab_f); cudaFree(pj.zent_f);
     pj = DevProjectors();
 }
 

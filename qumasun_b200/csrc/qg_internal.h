@@ -93,6 +93,12 @@ struct DevProjectors {
     std::vector<double> zk;  // k-vectors (3 per k-point) the tables were built for
     int zcap = 0;            // k-points the table buffers hold
     bool zready = false;
+    // the same tables in FP32 for complex64 states
+    float* ztab_f = nullptr;
+    float* zent_f = nullptr;
+    std::vector<double> zk_f;
+    int zcap_f = 0;
+    bool zready_f = false;
 };
 
 namespace qg {
@@ -215,13 +221,15 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
 
 // Complex k-point H (kpoint.cu): state s has its real part at X + s*ldx and its
 // imaginary part N elements later; coef_scratch holds 2*coef_scratch_elems(h, ns) doubles.
-int apply_hamiltonian_z(qg_hamiltonian h, int ns, const double* X, long long ldx, double* HX, long long ldhx,
-                        double* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
+template <typename T>
+int apply_hamiltonian_z(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
+                        T* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
 // Several k-points in one pass: nk k-vectors kv (3 each, bohr^-1), nsk states per k-point,
 // state s of k-point k at X + k*ldk + s*ldx (HX + k*ldkh + s*ldhx); coef_scratch holds
 // 2*coef_scratch_elems(h, nk*nsk) doubles.
-int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, const double* X, long long ldx,
-                         long long ldk, double* HX, long long ldhx, long long ldkh, double* coef_scratch,
-                         cudaStream_t st, PhaseTimer* pt = nullptr);
+template <typename T>
+int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, const T* X, long long ldx,
+                         long long ldk, T* HX, long long ldhx, long long ldkh, T* coef_scratch, cudaStream_t st,
+                         PhaseTimer* pt = nullptr);
 
 }  // namespace qg

@@ -500,7 +500,7 @@ bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc) {
     constexpr int PX = 16 / sizeof(T);
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
     if (nc != 1 && nc != 2) return false;
-    if (nc == 2 && (order != 8 || sizeof(T) != 8 || (a.xim % PX) || (a.hxim % PX))) return false;
+    if (nc == 2 && (order != 8 || (a.xim % PX) || (a.hxim % PX))) return false;
     if (a.row) return false;  // the nonlocal scatter runs in k_scatter_all on this path
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R)
@@ -518,10 +518,7 @@ int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc) 
     if (!stencil_tma_ok<T>(a, order, nc)) return QG_ERR_UNSUPPORTED;
     HamArgs<T> b = a;
     b.ty = tma_tile_rows(a, nc, order);
-    if (nc == 2) {
-        if constexpr (sizeof(T) == 8) return launch_order<T, 8, 2>(b, st);
-        return QG_ERR_UNSUPPORTED;
-    }
+    if (nc == 2) return launch_order<T, 8, 2>(b, st);
     switch (order) {
         case 2: return launch_order<T, 2, 1>(b, st);
         case 4: return launch_order<T, 4, 1>(b, st);

@@ -111,6 +111,9 @@ def lib():
         L.qg_hamiltonian_apply_host_z.argtypes = [vp, C.c_int, vp, vp]
         L.qg_hamiltonian_apply_zk.argtypes = [vp, C.c_int, _dp, C.c_int, vp, C.c_longlong, C.c_longlong, vp,
                                               C.c_longlong, C.c_longlong]
+        L.qg_hamiltonian_apply_zf.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
+        L.qg_hamiltonian_apply_zkf.argtypes = [vp, C.c_int, _dp, C.c_int, vp, C.c_longlong, C.c_longlong, vp,
+                                               C.c_longlong, C.c_longlong]
         L.qg_hamiltonian_apply_timed_z.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong,
                                                    C.POINTER(C.c_float)]
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
@@ -486,22 +489,27 @@ class Hamiltonian:
               "qg_hamiltonian_set_kvector")
 
     def apply_z(self, X, out=None):
-        """H_k X for a float64 torch CUDA tensor (ns, 2N) of split-complex states."""
+        """H_k X for a torch CUDA tensor (ns, 2N) of split-complex states: float64
+        (complex128 states) or float32 (complex64 states)."""
         import torch
-        assert X.is_cuda and X.dim() == 2 and X.shape[1] == 2 * self.N and X.dtype == torch.float64
+        assert X.is_cuda and X.dim() == 2 and X.shape[1] == 2 * self.N
+        assert X.dtype in (torch.float64, torch.float32)
         X = X.contiguous()
         if out is None:
             out = torch.empty_like(X)
         self.ctx.use_torch_stream()
-        check(lib().qg_hamiltonian_apply_z(self.h, X.shape[0], C.c_void_p(X.data_ptr()), 2 * self.N,
-                                           C.c_void_p(out.data_ptr()), 2 * self.N), "qg_hamiltonian_apply_z")
+        fn, name = ((lib().qg_hamiltonian_apply_z, "qg_hamiltonian_apply_z") if X.dtype == torch.float64
+                    else (lib().qg_hamiltonian_apply_zf, "qg_hamiltonian_apply_zf"))
+        check(fn(self.h, X.shape[0], C.c_void_p(X.data_ptr()), 2 * self.N, C.c_void_p(out.data_ptr()), 2 * self.N),
+              name)
         return out
 
     def apply_zk(self, kvecs, X, out=None):
         """H_k X for several k-points in one pass: X float64 CUDA tensor (nk, nsk, 2N),
         kvecs (nk, 3) Bloch vectors in bohr^-1."""
         import torch
-        assert X.is_cuda and X.dim() == 3 and X.shape[2] == 2 * self.N and X.dtype == torch.float64
+        assert X.is_cuda and X.dim() == 3 and X.shape[2] == 2 * self.N
+        assert X.dtype in (torch.float64, torch.float32)
         X = X.contiguous()
         kv = np.ascontiguousarray(np.asarray(kvecs, dtype=np.float64).reshape(-1, 3))
         assert kv.shape[0] == X.shape[0]
@@ -509,9 +517,10 @@ class Hamiltonian:
             out = torch.empty_like(X)
         self.ctx.use_torch_stream()
         nk, nsk = X.shape[0], X.shape[1]
-        check(lib().qg_hamiltonian_apply_zk(self.h, nk, kv.ctypes.data_as(_dp), nsk, C.c_void_p(X.data_ptr()),
-                                            2 * self.N, nsk * 2 * self.N, C.c_void_p(out.data_ptr()), 2 * self.N,
-                                            nsk * 2 * self.N), "qg_hamiltonian_apply_zk")
+        fn, name = ((lib().qg_hamiltonian_apply_zk, "qg_hamiltonian_apply_zk") if X.dtype == torch.float64
+                    else (lib().qg_hamiltonian_apply_zkf, "qg_hamiltonian_apply_zkf"))
+        check(fn(self.h, nk, kv.ctypes.data_as(_dp), nsk, C.c_void_p(X.data_ptr()), 2 * self.N, nsk * 2 * self.N,
+                 C.c_void_p(out.data_ptr()), 2 * self.N, nsk * 2 * self.N), name)
         return out
 
     def apply_host_z(self, X: np.ndarray, out: np.ndarray | None = None):
