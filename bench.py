@@ -473,8 +473,8 @@ def lobpcg_diamond216(ctx):
     """Time to the 480 lowest eigenpairs (528 solved, a 48-state guard band) of the
     216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
     kinetic-preconditioned GPU LOBPCG from the same seeded uniform(-0.5, 0.5) states:
-    FP64 Gram products against split-BF16x3 Gram products (QG_MIXED_BF16X3), which must
-    agree on the 480 eigenvalues to 1e-8 Ha."""
+    FP64 Gram products against split-BF16x3 (QG_MIXED_BF16X3) and FP32 (QG_FP32) Gram
+    products, which must agree on the 480 eigenvalues to 1e-8 Ha."""
     import numpy as np
     import torch
     from qumasun_b200 import Hamiltonian
@@ -486,7 +486,7 @@ def lobpcg_diamond216(ctx):
     X0 = torch.rand(ns, cell.N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
     runs = {}
     evs = {}
-    for name, prec in (("fp64", 0), ("bf16x3_gram", 2)):
+    for name, prec in (("fp64", 0), ("bf16x3_gram", 2), ("fp32_gram", 1)):
         X = X0.clone()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -504,9 +504,12 @@ def lobpcg_diamond216(ctx):
         del X
     H.close()
     diff = float(np.abs(evs["fp64"] - evs["bf16x3_gram"]).max())
+    diff32 = float(np.abs(evs["fp64"] - evs["fp32_gram"]).max())
     return {"workload": "diamond216_120cube_480of528states_fd8_kinetic_precond", **runs,
             "max_abs_ev_diff_mixed_vs_fp64_Ha": diff,
-            "speedup_mixed_vs_fp64": round(runs["fp64"]["seconds"] / runs["bf16x3_gram"]["seconds"], 3)}
+            "max_abs_ev_diff_fp32_gram_vs_fp64_Ha": diff32,
+            "speedup_mixed_vs_fp64": round(runs["fp64"]["seconds"] / runs["bf16x3_gram"]["seconds"], 3),
+            "speedup_fp32_gram_vs_fp64": round(runs["fp64"]["seconds"] / runs["fp32_gram"]["seconds"], 3)}
 
 
 # --------------------------------------------------------------- GPU arm

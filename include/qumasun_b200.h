@@ -199,7 +199,9 @@ typedef struct qg_lobpcg_options {
     double tol;         /* stop when max_j sum_i r_j(i)^2 dV < tol * dV (reference limit 1e-10,
                            lobpcg_d_multi.h:54, :525); <= 0 selects 1e-10 */
     int first_call;     /* 1: start with P = 0 and the 2n x 2n first step (reference is_first_time) */
-    int precision;      /* QG_FP64: FP64 throughout; QG_MIXED_BF16X3: split-BF16x3 Gram products */
+    int precision;      /* QG_FP64: FP64 throughout; QG_MIXED_BF16X3: split-BF16x3 Gram products;
+                           QG_FP32: FP32 Gram products (chunked, FP64 across chunks); both reduced
+                           modes hand over to FP64 Gram products near convergence */
     int verbose;        /* 1: print (iteration, max residual) lines to stdout */
     int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
                            applied in Fourier space with the FD stencil's own symbol; 2: kinetic
@@ -289,7 +291,8 @@ int qg_lobpcg_cells_device(int ncells, const qg_hamiltonian* hams, const qg_lobp
  * ld N; B NULL means B = A) through the mixed-precision Gram of QG_MIXED_BF16X3:
  * pieces = 2 or 3 bf16 pieces per value on the library's tcgen05 kernel (FP32
  * accumulation over one 64-row K block, FP64 across blocks; N a multiple of 8),
- * pieces = 0 the cuBLAS BF16 hi/lo path (FP32 over 1024-row chunks). Waits for
+ * pieces = 0 the cuBLAS BF16 hi/lo path (FP32 over 1024-row chunks), pieces = -1
+ * FP32 copies and FP32 GEMMs over the same chunks (the Gram of QG_FP32). Waits for
  * the stream; returns QG_ERR_UNSUPPORTED if the tcgen05 path cannot take N. */
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
                     double* C, int pieces);

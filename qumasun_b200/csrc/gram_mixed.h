@@ -18,7 +18,8 @@ struct MixedGram {
     int mmax = 0, nfull = 0, rem = 0;
     DevBuf split_a, split_b, part;
     // pieces > 0: the tcgen05 kernel with that many bf16 pieces (gram_tc.cu);
-    // 0 (or a row count that is not a multiple of 8): cuBLAS BF16 GEMMs on hi/lo pieces
+    // 0 (or a row count that is not a multiple of 8): cuBLAS BF16 GEMMs on hi/lo pieces;
+    // -1: FP32 copies and FP32 GEMMs (no tensor cores, no TF32)
     int pieces = 3;
     bool use_tc = false;
     TcGram tc;
@@ -30,6 +31,7 @@ struct MixedGram {
     // only the lower triangle is needed (the tcgen05 kernel then skips the upper tiles)
     int gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, double* C,
              int ldc, int* err);
+    int gram_fp32(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, double alpha, double* C, int ldc);
     void release();
     ~MixedGram() { release(); }
 };

@@ -356,7 +356,8 @@ struct Solver {
     double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *Sa, *Sb, *Sa2, *Sb2, *M;
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
     std::vector<double> s_h;
-    bool mixed = false;      // split-BF16x3 Gram products (qg::MixedGram)
+    bool mixed = false;      // reduced-precision Gram products (qg::MixedGram) until the hand-over
+    int mixed_pieces = 3;    // qg::MixedGram split: 3 = split-BF16x3 on tcgen05, -1 = FP32
     double trunc_eps = 1e-12;  // relative eigenvalue floor of B in the rank-revealing solve
     qg::MixedGram mg;
     cuDoubleComplex *Ca, *Cb;
@@ -413,7 +414,7 @@ struct Solver {
         }
         QG_TRY(h->coef.reserve((c == 1 ? qg::coef_scratch_elems(h, n) : qg::coef_scratch_elems_z(h, 1, n)) *
                                sizeof(double)));
-        if (mixed) QG_TRY(mg.setup(N, (int)g3));
+        if (mixed) QG_TRY(mg.setup(N, (int)g3, mixed_pieces));
         return QG_OK;
     }
 
@@ -626,7 +627,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
     if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
     if (comps == 2 && h->order != 8) return QG_ERR_UNSUPPORTED;
-    if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3) return QG_ERR_UNSUPPORTED;
+    if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3 && opt->precision != QG_FP32)
+        return QG_ERR_UNSUPPORTED;
     if (opt->precond < 0 || opt->precond > 2) return QG_ERR_INVALID;
     if (opt->precond == 2 && !h->learned) return QG_ERR_INVALID;
     const long long N = h->N();
@@ -640,7 +642,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     s.L = comps * N;
     s.dV = h->hx * h->hy * h->hz;
     s.st = h->ctx->stream;
-    s.mixed = opt->precision == QG_MIXED_BF16X3;
+    s.mixed = opt->precision == QG_MIXED_BF16X3 || opt->precision == QG_FP32;
+    s.mixed_pieces = opt->precision == QG_FP32 ? -1 : 3;
     s.trunc_eps = s.mixed ? 1e-6 : 1e-12;
     QG_TRY(qg_blas_handle(h->ctx, &s.blas));
     QG_TRY(qg_solver_handle(h->ctx, &s.sol));

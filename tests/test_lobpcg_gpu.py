@@ -76,8 +76,9 @@ def test_kinetic_preconditioner_same_eigenpairs_fewer_iterations(cuda_ctx):
     assert r["report"]["iterations"] < int(g["iters"]) // 3
 
 
-def test_mixed_precision_gram_reaches_fp64_eigenvalues(cuda_ctx):
-    """Split-BF16x3 Gram products (precision QG_MIXED_BF16X3) with the FP64
+@pytest.mark.parametrize("precision", [2, 1], ids=["bf16x3", "fp32"])
+def test_mixed_precision_gram_reaches_fp64_eigenvalues(cuda_ctx, precision):
+    """Split-BF16x3 (QG_MIXED_BF16X3) or FP32 (QG_FP32) Gram products with the FP64
     residual and the final FP64 Rayleigh-Ritz: the same 16 eigenvalues as the
     reference solver to 1e-8 Ha on the 8-atom 40^3 cell."""
     import torch
@@ -87,9 +88,10 @@ def test_mixed_precision_gram_reaches_fp64_eigenvalues(cuda_ctx):
     X0 = initial_states(int(g["ns"]), cell.N, seed=int(g["seed"]))
     H = Hamiltonian(cuda_ctx, cell)
     X = torch.from_numpy(X0).cuda()
-    r = H.lobpcg_device(X, None, max_iter=400, precond=1, precision=2)
+    r = H.lobpcg_device(X, None, max_iter=400, precond=1, precision=precision)
     H.close()
     assert r["status"] == 0 and r["report"]["converged"] == 1
+    assert r["report"]["mixed_iterations"] > 0
     np.testing.assert_allclose(np.sort(r["ev"]), np.sort(g["ev"]), rtol=0, atol=1e-8)
 
 
