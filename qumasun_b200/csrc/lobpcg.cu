@@ -860,8 +860,6 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
 // DGEMMs over k; the small Hermitian pencils are solved k by k
 // (Jacobi-equilibrated cusolverDnZhegvd, the rank-revealing solve where B is
 // singular). Stops when every k-point's lowest n_converge states meet tol.
-constexpr bool kHegBatched = true;
-constexpr double kHegPivotFloor = 0.0;
 // k-points whose largest residual (sum r^2 dV, the convergence measure) is below this
 // times dV take zhegvd instead of the batched Jacobi solver: on the 8-atom 40^3 cell
 // (64 k-points, 16 states) the two give the same iterates down to ~1e-5 and the
@@ -929,7 +927,7 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
     // pencils of up to kSmallHegMax rows: all k-points' Hermitian pencils in one launch
     // of the one-block Jacobi solver (small_eig.cu), cuSOLVER's zhegvd per k-point
     // otherwise and for any pencil the Jacobi solver rejects
-    const bool batched_eig = k3m <= qg::kSmallHegMax && kHegBatched;
+    const bool batched_eig = k3m <= qg::kSmallHegMax;
     DevBuf& heg = s.heg;
     cuDoubleComplex *CaAll = nullptr, *CbAll = nullptr;
     double* wAll = nullptr;
@@ -1033,24 +1031,21 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
             // the pencils of nearly converged k-points (residual below kJacobiResidual,
             // nearly singular B) go to zhegvd one by one, with which the iteration
             // converges in fewer steps
-            int n_jac = 0;
             for (int k = 0; k < nk; ++k) {
                 double mk = it == 0 ? 1e300 : 0.0;
                 if (it > 0)
                     for (int j = 0; j < nconv; ++j) mk = std::max(mk, nr_h[k * nb + j]);
                 near[k] = !frozen[k] && mk < kJacobiResidual * s.dV;
                 skip_h[k] = (frozen[k] || near[k]) ? 1 : 0;
-                n_jac += skip_h[k] ? 0 : 1;
             }
             QG_CUDA_TRY(cudaMemcpyAsync(skip_d, skip_h.data(), nk * sizeof(int), cudaMemcpyHostToDevice, st));
             k_gram_to_complex_b<<<dim3(k3, nk), 128, 0, st>>>(SaAll, SbAll, g, (long long)gsz, k3, CaAll, CbAll, k3,
                                                                (long long)kk, skip_d);
             QG_TRY(qg::small_heg_launch(reinterpret_cast<const double2*>(CaAll), reinterpret_cast<const double2*>(CbAll),
                                         k3, (long long)kk, k3, skip_d, reinterpret_cast<double2*>(CaAll), k3,
-                                        (long long)kk, wAll, k3m, infos_d, nk, st, kHegPivotFloor));
+                                        (long long)kk, wAll, k3m, infos_d, nk, st));
             k_expand_rotation_b<<<dim3(nb, nk), 128, 0, st>>>(CaAll, k3, (long long)kk, k3, SbAll, g, (long long)gsz,
                                                                Mall, g, (long long)msz, skip_d);
-            (void)n_jac;
             for (int k = 0; k < nk; ++k) {
                 if (!near[k]) continue;
                 double* Sa_k = SaAll + k * gsz;
