@@ -231,7 +231,11 @@ def lobpcg_cells(hams, Xs, Ps=None, max_iter=2000, tol=1.0e-10, first=True, prec
     assert n == len(Xs) and len({id(h.ctx) for h in hams}) == n, "one context per cell"
     for X in Xs:
         assert X.is_cuda and X.dtype == torch.float64 and X.is_contiguous()
-    streams = [torch.cuda.Stream(device=X.device) for X in Xs]
+    # the costliest cells (grid points x states, the top half) run on high-priority
+    # streams: their solves are the critical path, the small cells fill the gaps
+    cost = [X.shape[0] * X.shape[1] for X in Xs]
+    cut = sorted(cost)[len(cost) // 2]
+    streams = [torch.cuda.Stream(device=X.device, priority=-1 if c >= cut else 0) for X, c in zip(Xs, cost)]
     torch.cuda.synchronize()  # inputs written on other streams are complete
     for h, s in zip(hams, streams):
         h.ctx.set_stream(s.cuda_stream)
