@@ -297,6 +297,14 @@ int qg_lobpcg_cells_device(int ncells, const qg_hamiltonian* hams, const qg_lobp
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
                     double* C, int pieces);
 
+/* The Gram product the real LOBPCG uses for pencils of up to 128 columns
+ * (MakeMatrix_d_blas, lobpcg_d_multi_mpi.h:191-250, with K = the grid): C (ma x mb,
+ * column-major, ld ma) = alpha * A^T B for DEVICE blocks A (N x ma) and B (N x mb),
+ * ld N, with K split over the GPU and the partial sums added in a fixed order. Any
+ * ma, mb (64 x 64 output tiles); waits for the stream. */
+int qg_gram_small_d(qg_context ctx, long long N, int ma, int mb, const double* A, const double* B, double alpha,
+                    double* C);
+
 /* ---- learned preconditioner ------------------------------------------------
  * No counterpart in the reference (its solvers are unpreconditioned). A 4-layer
  * periodic 3D convolutional network (3^3 kernels, channels 2 -> 16 -> 16 -> 16 -> 1,

@@ -13,6 +13,8 @@
 #include "gram_ts.h"
 #include "qg_internal.h"
 
+#include <algorithm>
+
 namespace qg {
 namespace {
 
@@ -159,3 +161,18 @@ int gram_ts_tiled(const double* A, long long lda, long long sA, const double* B1
 }
 
 }  // namespace qg
+
+extern "C" int qg_gram_small_d(qg_context ctx, long long N, int ma, int mb, const double* A, const double* B,
+                               double alpha, double* C) {
+    if (!ctx || N <= 0 || ma <= 0 || mb <= 0 || !A || !B || !C) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaSetDevice(ctx->device));
+    double* scratch = nullptr;
+    const size_t bytes = qg::gram_ts_scratch_doubles(N, 1, false) * sizeof(double);
+    QG_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, ctx->stream));
+    const int rc = qg::gram_ts_tiled(A, N, 0, B, nullptr, N, 0, N, ma, mb, alpha, C, nullptr, ma, 0, 1, scratch,
+                                     ctx->stream);
+    cudaFreeAsync(scratch, ctx->stream);
+    if (rc != QG_OK) return rc;
+    QG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return QG_OK;
+}

@@ -124,6 +124,7 @@ def lib():
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
         L.qg_sygv_small_batched_d.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
         L.qg_hegv_small_batched_z.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, C.c_longlong, vp, vp, _ip]
+        L.qg_gram_small_d.argtypes = [vp, C.c_longlong, C.c_int, C.c_int, vp, vp, C.c_double, vp]
         L.qg_lobpcg_d.argtypes = [vp, C.POINTER(LobpcgOptions), C.c_int, _dp, vp, vp, C.POINTER(LobpcgReport)]
         L.qg_gram_mixed_d.argtypes = [vp, C.c_longlong, C.c_int, vp, vp, C.c_double, vp, C.c_int]
         L.qg_learned_create.argtypes = [vp, C.POINTER(vp)]
