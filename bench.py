@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--sweep", action="store_true", help="also time FD orders 2/4/6 and FP32")
+    p.add_argument("--no-sweep", action="store_true", help="skip the FD order 2/4/6/8 x FP64/FP32 sweep")
     p.add_argument("--no-lobpcg", action="store_true", help="skip the LOBPCG time-to-solution legs")
     p.add_argument("--no-lobpcg216", action="store_true",
                    help="skip the 216-atom 120^3 LOBPCG leg (FP64 vs BF16x3 Gram, about a minute)")
@@ -605,7 +605,7 @@ def run_gpu_arm(a):
                "d2h_bytes_per_step": NS * N * 8, "seconds_per_step": round(e2e_s, 5)}
 
     sweep = {}
-    if a.sweep and rank == 0:
+    if not a.no_sweep and rank == 0:
         for order in (2, 4, 6, 8):
             Ho = Hamiltonian(ctx, cell, fd_order=order)
             for dt in ("f64", "f32"):
