@@ -455,9 +455,8 @@ template <typename T, int ORDER, int NC, int NXC = 0>
 int launch_order(const HamArgs<T>& a, cudaStream_t st) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = radius<ORDER>();
-    if constexpr (NXC == 0 && ORDER == 8 && sizeof(T) == 8) {
-        // FP64 order 8 (the reference's default): row lengths of the common grids
-        // compiled in
+    if constexpr (NXC == 0 && ORDER >= 4) {
+        // orders 4-8, FP64 and FP32: row lengths of the common grids compiled in
         switch (a.nx) {
             case 40: return launch_order<T, ORDER, NC, 40>(a, st);
             case 80: return launch_order<T, ORDER, NC, 80>(a, st);
