@@ -6,7 +6,7 @@
 // cuBLAS spends milliseconds on these shapes (an m x m output has too few tiles to
 // spread K = 64k-1.7M rows over the GPU). Here K is split: block b sums rows
 // [b*rows, (b+1)*rows) in shared-memory chunks of 24 rows, each thread holding a
-// 4 x 4 tile of the (up to) 64 x 64 output, for one or two right-hand blocks at once
+// 4 x 4 (or, up to 32 columns, 2 x 2) tile of the output, for one or two right-hand blocks at once
 // (A^T B1 and A^T B2 share the reads of A); a second kernel adds the per-block
 // partial sums in block order (deterministic) and scales by alpha. Several
 // problems (blockIdx.y) run in one launch.
@@ -22,6 +22,7 @@ constexpr int kRows = 24;   // rows per shared-memory chunk (3 x 24 x 65 doubles
 constexpr int kT = 16;      // 16 x 16 threads, 4 x 4 outputs each
 constexpr int kMax = 64;
 
+template <int TILE>
 __global__ void __launch_bounds__(kT * kT) k_gram_ts_partial(const double* __restrict__ A, long long lda,
                                                              long long sA, const double* __restrict__ B1,
                                                              const double* __restrict__ B2, long long ldb,
@@ -38,13 +39,13 @@ __global__ void __launch_bounds__(kT * kT) k_gram_ts_partial(const double* __res
     const int ti = t / kT, tj = t % kT;
     const long long r0 = (long long)blockIdx.x * rows_per_block;
     const long long r1 = min(N, r0 + rows_per_block);
-    double acc[2][4][4];
+    double acc[2][TILE][TILE];
 #pragma unroll
     for (int q = 0; q < 2; ++q)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < TILE; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[q][i][j] = 0.0;
+            for (int j = 0; j < TILE; ++j) acc[q][i][j] = 0.0;
     for (long long rc = r0; rc < r1; rc += kRows) {
         const int nr = (int)min((long long)kRows, r1 - rc);
         // column-wise coalesced loads: consecutive rows of one column per warp
@@ -60,18 +61,18 @@ __global__ void __launch_bounds__(kT * kT) k_gram_ts_partial(const double* __res
         __syncthreads();
 #pragma unroll 4
         for (int rr = 0; rr < kRows; ++rr) {
-            double a[4], b[4];
+            double a[TILE], b[TILE];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[rr][ti * 4 + i];
+            for (int i = 0; i < TILE; ++i) a[i] = As[rr][ti * TILE + i];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 if (q >= nb) break;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[q][rr][tj * 4 + j];
+                for (int j = 0; j < TILE; ++j) b[j] = Bs[q][rr][tj * TILE + j];
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < TILE; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[q][i][j] += a[i] * b[j];
+                    for (int j = 0; j < TILE; ++j) acc[q][i][j] += a[i] * b[j];
             }
         }
         __syncthreads();
@@ -83,10 +84,10 @@ __global__ void __launch_bounds__(kT * kT) k_gram_ts_partial(const double* __res
     for (int q = 0; q < 2; ++q) {
         if (q >= nb) break;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < TILE; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int ii = ti * 4 + i, jj = tj * 4 + j;
+            for (int j = 0; j < TILE; ++j) {
+                const int ii = ti * TILE + i, jj = tj * TILE + j;
                 if (ii < ma && jj < mb) pb[(long long)q * msz + ii * mb + jj] = acc[q][i][j];
             }
     }
@@ -135,8 +136,13 @@ int gram_ts(const double* A, long long lda, long long sA, const double* B1, cons
     if (ma <= 0 || mb <= 0 || ma > kMax || mb > kMax || N <= 0 || nprob <= 0) return QG_ERR_UNSUPPORTED;
     const int nblocks = gram_ts_blocks(N, nprob);
     const long long rows = (N + nblocks - 1) / nblocks;
-    k_gram_ts_partial<<<dim3(nblocks, nprob), kT * kT, 0, st>>>(A, lda, sA, B1, B2, ldb, sB, N, ma, mb, rows,
-                                                                 scratch);
+    // 2 x 2 outputs per thread when both sides fit 32 columns (every thread busy)
+    if (ma <= 2 * kT && mb <= 2 * kT)
+        k_gram_ts_partial<2><<<dim3(nblocks, nprob), kT * kT, 0, st>>>(A, lda, sA, B1, B2, ldb, sB, N, ma, mb, rows,
+                                                                        scratch);
+    else
+        k_gram_ts_partial<4><<<dim3(nblocks, nprob), kT * kT, 0, st>>>(A, lda, sA, B1, B2, ldb, sB, N, ma, mb, rows,
+                                                                        scratch);
     const int nb = B2 ? 2 : 1;
     const int tot = nb * ma * mb;  // one warp each, 8 warps per block
     k_gram_ts_reduce<<<dim3((tot + 7) / 8, nprob), 256, 0, st>>>(scratch, nblocks, nb, ma, mb, alpha, C1, C2, ldc,
