@@ -604,8 +604,13 @@ def run_gpu_arm(a):
         e2e = {"value": round(nbytes * ws / e2e_s / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": NS * N * 8,
                "d2h_bytes_per_step": NS * N * 8, "seconds_per_step": round(e2e_s, 5)}
 
+    # the legs that only rank 0 runs (sweep, learned, LOBPCG, cells) run in single-GPU
+    # runs only: with several ranks the others would wait at the final barrier for longer
+    # than the process group's timeout; the multi-GPU line carries the headline metric and
+    # the sharded k-point leg
+    solo = ws == 1
     sweep = {}
-    if not a.no_sweep and rank == 0:
+    if not a.no_sweep and solo:
         for order in (2, 4, 6, 8):
             Ho = Hamiltonian(ctx, cell, fd_order=order)
             for dt in ("f64", "f32"):
@@ -644,14 +649,14 @@ def run_gpu_arm(a):
     if not a.no_kpoint:
         kp = kpoint_leg(ctx, n_k=a.kpoints, rank=rank, ws=ws)
     lrn = None
-    if rank == 0 and not a.no_learned:
+    if solo and not a.no_learned:
         lrn = learned_leg(ctx)
     cells_res = None
-    if rank == 0 and not a.no_cells:
+    if solo and not a.no_cells:
         cells_res = cells_leg()
     lob = None
     lob216 = None
-    if rank == 0 and not a.no_lobpcg:
+    if solo and not a.no_lobpcg:
         lob = lobpcg_diamond8(ctx, cpu=(ws == 1 and not a.no_cpu_baseline))
         if not a.no_lobpcg216:
             del X, HX
