@@ -175,19 +175,21 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian ham, int ns, const double* X, lo
                                  double* HX, long long ldhx, float* ms_phases);
 /* No counterpart in the reference (its CPU operator allocates freely).
  * Same result as qg_hamiltonian_apply_d (FP64, DEVICE pointers, context
- * stream), for callers that cannot allocate device memory at the point of the
- * call: work being recorded into a CUDA stream capture, loops that must not
- * touch the allocator, hosts whose device memory belongs to another framework.
- * It allocates nothing: the projector coefficients go to a scratch array
- * compiled into the library, qg_noalloc_scratch_capacity() doubles (4 MiB) per
- * device, which must hold ns16 * n_atoms * n_channels values (ns16 = ns rounded
- * up to a multiple of 16; n_channels = 4 for s+p projectors); larger batches
- * return QG_ERR_UNSUPPORTED. The first call on
- * a device looks up the array's device address (a CUDA runtime query, no
- * allocation), so make that first call before any stream capture. All calls
- * on a device share the array and it keeps the last call's contents (each call
- * overwrites every slot it reads before reading it): calls that overlap on the
- * GPU (other streams, other threads) race and must be serialised by the caller. */
+ * stream), for callers that cannot call cudaMalloc at the point of the call:
+ * hosts whose device memory belongs to another framework's allocator (a pool
+ * that must not be bypassed), and time-critical loops that must not touch the
+ * allocator. It allocates nothing: the projector coefficients go to a scratch
+ * array compiled into the library, qg_noalloc_scratch_capacity() doubles
+ * (4 MiB) per device that loads the library, held until the process exits,
+ * which must hold ns16 * n_atoms * n_channels values (ns16 = ns rounded up to a
+ * multiple of 16; n_channels = 4 for s+p projectors); larger batches return
+ * QG_ERR_UNSUPPORTED before anything is launched. The first call on a device
+ * looks up the array's device address (a CUDA runtime query, no allocation), so
+ * make that first call before any stream capture. All calls on a device share
+ * the array and it keeps the last call's contents: each call writes the slots
+ * [0, ns) of every coefficient row before reading them; the padding slots
+ * [ns, ns16) may be read but never reach HX. Calls that overlap on the GPU
+ * (other streams, other threads) race and must be serialised by the caller. */
 int qg_hamiltonian_apply_noalloc_d(qg_hamiltonian ham, int ns, const double* X, long long ldx,
                                    double* HX, long long ldhx);
 /* Capacity, in doubles, of the fixed scratch array qg_hamiltonian_apply_noalloc_d uses. */

@@ -1,10 +1,9 @@
 // H|psi> without any allocation inside the call.
 //
 // Some callers cannot call cudaMalloc at the point where they need H|psi>:
-// code issuing work into a CUDA stream capture (allocation is not a
-// capturable stream operation), time-critical loops that must not touch the
-// allocator, and host programs whose device memory is owned by another
-// framework's allocator. qg_hamiltonian_apply_d grows a per-operator scratch
+// host programs whose device memory is owned by another framework's allocator
+// (a pool that must not be bypassed), and time-critical loops that must not
+// touch the allocator. qg_hamiltonian_apply_d grows a per-operator scratch
 // buffer for the projector coefficients on first use; this entry point
 // instead uses a fixed buffer compiled into the library (below), so the call
 // itself allocates nothing. The operator handle (built earlier, outside the

@@ -20,6 +20,7 @@
 // records QG_ERR_TIMEOUT in the device status word and the block winds down:
 // consumers stop, the producer stops issuing, and after a final block barrier
 // the producer lane waits (bounded) for its copies still in flight.
+#include <atomic>
 #include <cstdint>
 
 #include "qg_internal.h"
@@ -441,13 +442,20 @@ int ring_stages_for(int R, size_t stage_bytes) {
     return nst >= need ? nst : -1;
 }
 
+// SM count of the current device, looked up once per device (devices of one process
+// may differ: MIG slices, mixed parts). Racing first lookups store the same value.
 int sm_count() {
-    static const int n = [] {  // initialised once, also when several host threads launch
-        int dev = 0, c = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
-        return c > 0 ? c : 148;
-    }();
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> cache[kMaxDev];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDev) dev = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+    int c = 0;
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+    n = c > 0 ? c : 148;
+    cache[dev].store(n, std::memory_order_relaxed);
     return n;
 }
 

@@ -387,23 +387,47 @@ class Hamiltonian:
         check(fn(self.h, ns, C.c_void_p(x_ptr), ldx, C.c_void_p(hx_ptr), ldhx),
               "qg_hamiltonian_apply_" + ("d" if dtype == "f64" else "f"))
 
+    def _check_block(self, X, name, dtypes):
+        """A state block the kernels may read or write whole: a contiguous CUDA tensor
+        (ns, N) of one of `dtypes` on this context's device."""
+        import torch
+        if not isinstance(X, torch.Tensor) or not X.is_cuda:
+            raise TypeError(f"{name} must be a CUDA tensor")
+        if X.dtype not in dtypes:
+            raise TypeError(f"{name} has dtype {X.dtype}, expected one of {dtypes}")
+        if X.dim() != 2 or X.shape[1] != self.N:
+            raise ValueError(f"{name} has shape {tuple(X.shape)}, expected (ns, {self.N})")
+        if not X.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+        if X.device.index != self.ctx.device:
+            raise ValueError(f"{name} is on cuda:{X.device.index}, the operator on cuda:{self.ctx.device}")
+
     def apply(self, X, out=None):
         """HX = H X for torch CUDA tensors (ns, N) of float64 or float32."""
         import torch
-        assert X.is_cuda and X.dim() == 2 and X.shape[1] == self.N
+        self._check_block(X.contiguous() if isinstance(X, torch.Tensor) else X, "X",
+                          (torch.float64, torch.float32))
         X = X.contiguous()
         if out is None:
             out = torch.empty_like(X)
+        self._check_block(out, "out", (X.dtype,))
+        if out.shape != X.shape:
+            raise ValueError(f"out has shape {tuple(out.shape)}, X {tuple(X.shape)}")
         dt = "f64" if X.dtype == torch.float64 else "f32"
-        if dt == "f32" and X.dtype != torch.float32:
-            raise TypeError("states must be float64 or float32")
         self.ctx.use_torch_stream()
         self.apply_device(X.shape[0], X.data_ptr(), out.data_ptr(), dtype=dt)
         return out
 
     def apply_noalloc(self, X, out):
         """HX = H X (FP64 torch CUDA tensors) through the entry point that allocates
-        nothing: the projector coefficients use the library's fixed scratch array."""
+        nothing: the projector coefficients use the library's fixed scratch array.
+        X and out must be contiguous float64 CUDA tensors of the same shape (ns, N) on
+        the operator's device; anything else raises before the library is called."""
+        import torch
+        self._check_block(X, "X", (torch.float64,))
+        self._check_block(out, "out", (torch.float64,))
+        if out.shape != X.shape:
+            raise ValueError(f"out has shape {tuple(out.shape)}, X {tuple(X.shape)}")
         self.ctx.use_torch_stream()
         check(lib().qg_hamiltonian_apply_noalloc_d(self.h, X.shape[0], C.c_void_p(X.data_ptr()), self.N,
                                                    C.c_void_p(out.data_ptr()), self.N),
