@@ -91,6 +91,8 @@ typedef struct qg_hamiltonian_desc {
 
 /* ---- status / context -------------------------------------------------- */
 const char* qg_status_string(int status);
+/* Text of the last error the library recorded on this host thread's calls (empty if none). */
+const char* qg_last_error(void);
 int qg_version(void);
 
 /* Creates a context on CUDA device `device` with its own non-blocking stream.
@@ -358,10 +360,14 @@ int qg_sygv_small_batched_d(qg_context ctx, int batch, int k, const double* A, c
 int qg_hegv_small_batched_z(qg_context ctx, int batch, int k, const double* A, const double* B, int lda,
                             long long stride, double* w, double* Z, int* info);
 
-/* Selects the stencil kernel of an operator: 0 = the TMA-staged ring kernel
- * where the shape and alignment allow (default), 1 = always the
- * register-window kernel (any shape). Both compute the same operator. */
-int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int plain);
+/* Selects the stencil kernel of an operator's real-state apply: 0 = the engine's
+ * choice (default: the one-plane TMA ring kernel where the shape and alignment
+ * allow, else the two-plane ring kernel, else the register-window kernel),
+ * 1 = always the register-window kernel (any shape), 2 = the one-plane ring
+ * kernel, 3 = the two-plane ring kernel (2 and 3 fall back as 0 does where the
+ * shape does not fit). All compute the same operator. Complex states use the
+ * one-plane ring kernel unless 1 is set. */
+int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int variant);
 /* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
  * complex states use at most 4), states per scatter group of the real apply (4 or
  * 8), and blocks per atom in the projection (1-8, one thread-block cluster; the
@@ -374,6 +380,71 @@ int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian ham, int project_states,
                                          int project_parts);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
+
+/* ---- SCF-step neighbours of the eigensolver ---------------------------- */
+
+/* rho[i] (+)= sum_s occ[s] * psi_s[i]^2 over the states with occ[s] > 0, in state
+ * order, each term rounded as the reference forms it ((psi*psi)*occ added to rho, no
+ * fused multiply-add): the sums equal the reference's bit for bit on the same inputs.
+ * X: ns real states on the DEVICE, state s at X + s*ldx (ldx >= N); occ: HOST, ns
+ * values; rho: DEVICE, N values, zeroed first unless accumulate != 0. Context stream;
+ * returns after the kernel has run. Replaces QUMASUN_SINGLE::mSetDensityOne
+ * (qumasun_single.density.h:10-27). */
+int qg_density_d(qg_context ctx, long long N, int ns, const double* X, long long ldx, const double* occ,
+                 double* rho, int accumulate);
+/* Complex {re[N], im[N]} states (ldx >= 2N): rho += occ * (re^2 + im^2). Replaces
+ * QUMASUN_KPOINT::mSetDensityOne (qumasun_kpoint.density.h:11-33). */
+int qg_density_z(qg_context ctx, long long N, int ns, const double* X, long long ldx, const double* occ,
+                 double* rho, int accumulate);
+/* Fermi occupations (2 electrons per state) of n eigenvalues (HOST, ascending) for
+ * n_electrons electrons at temperature kbT (Ha): bisection on the chemical potential
+ * from [ev[0], 16 |ev[n-1]|-ish] down to 1e-9 Ha, occ[s] = 2/(exp(min((ev-mu)/kbT, 80))+1).
+ * HOST arithmetic (a few hundred exponentials per step). Replaces
+ * QUMASUN_SINGLE::mSetOccupancySpinOff (qumasun_single.occupancy.h:19-55) with
+ * SetOccupancy (SetOccupancy.h:7-18). */
+int qg_occupancy(double kbT, int n, const double* ev, int n_electrons, double* occ, double* mu);
+/* Spin-polarised form: one state per electron in each spin channel, one shared mu.
+ * Replaces mSetOccupancySpinOn (qumasun_single.occupancy.h:62-109). */
+int qg_occupancy_spin(double kbT, int n, const double* ev_up, const double* ev_dn, int n_electrons,
+                      double* occ_up, double* occ_dn, double* mu);
+
+typedef struct qg_poisson_s* qg_poisson;
+/* FFT Poisson + LDA potential builder for an nx x ny x nz periodic grid of spacing
+ * (hx, hy, hz): owns a cuFFT plan and an N-point complex buffer on the context's device.
+ * The context must outlive it. */
+int qg_poisson_create(qg_context ctx, int nx, int ny, int nz, double hx, double hy, double hz, qg_poisson* out);
+int qg_poisson_destroy(qg_poisson p);
+/* V_tot = V_ext + V_hart + V_x + V_c on the DEVICE (context stream), all arrays of N
+ * doubles: V_hart from the periodic Poisson equation solved by FFT, 4 pi/|k|^2 on the
+ * folded wave numbers with the k = 0 term dropped, inverse transform scaled by 1/N;
+ * V_x, V_c the Perdew-Zunger 1981 LDA potentials of rho + pcc (zero below 1e-8).
+ * pcc may be NULL (no core charge); vhart, vx, vc may be NULL (not returned).
+ * Replaces QUMASUN_SINGLE::mSetPotential for KohnSham_PP without spin
+ * (qumasun_single.potential.h:33-43): mSetPotentialVhart (:101-200, the same solve as
+ * SetPotentialByPoissonFFT, poisson_fft.h:14-128) and mSetPotentialVxc (:311-317,
+ * Calc_XC_LDA, Vxc.h:41-70). */
+int qg_potential_lda_d(qg_poisson p, const double* rho, const double* pcc, const double* vext, double* vtot,
+                       double* vhart, double* vx, double* vc);
+
+/* One fourth-order Taylor step psi <- sum_{j=0..4} (-i dt H)^j / j! psi of ns complex
+ * {re[N], im[N]} states (DEVICE, in place, ldx >= 2N) under the operator at its
+ * k-vector (FD order 8): four applications of H to the whole block, each followed by
+ * the update of that order. Work: two blocks of ns states kept by the operator.
+ * Replaces QUMASUN::TimeEvoH4 (qumasun_td.time_evo_H4.h:13-60), which steps one state
+ * at a time. */
+int qg_td_taylor4_z(qg_hamiltonian ham, int ns, double dt, double* X, long long ldx);
+
+/* Nonlocal energy and forces of ns real states (DEVICE X, state s at X + s*ldx): for
+ * every state, inner = dV <p|psi> over all projector channels and e_state[s] =
+ * sum E inner^2 (EnergyPPnonlocal, PseudoPotOperator.h:775-816); for the states with
+ * occ[s] > 0, dpsi = -2 occ grad psi (8th-order FD gradient, Gradient8th,
+ * GridGradient8th.h:19-235), dinner = dV <p|dpsi> and forces[3a + d] +=
+ * sum E inner dinner_d; *ev_sum = sum occ[s] e_state[s]. occ, forces (3 per atom,
+ * accumulated), e_state (may be NULL) and ev_sum (may be NULL) are HOST. Replaces
+ * QUMASUN_MPI::mGetForcePseudoNonlocal (qumasun_mpi.force.h:227-254) with
+ * PseudoPotIntegrator_mpi::ForceNonlocal (PseudoPotOperator_mpi_v2.h:905-1010). */
+int qg_nonlocal_force_d(qg_hamiltonian ham, int ns, const double* X, long long ldx, const double* occ,
+                        double* forces, double* e_state, double* ev_sum);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,16 @@ inline int lapack_DSYGVX(double* A, double* B, double* ev, double* evec, double*
 #undef private
 #undef protected
 
+/* SCF-step neighbours of the eigensolver: the FFT Poisson solve (poisson_fft.h, FFTW
+ * provided by shims/fftw3.h), LDA exchange-correlation (Vxc.h), Fermi occupations
+ * (SetOccupancy.h), the 8th-order gradient (GridGradient8th.h) and the Taylor-4
+ * propagator (qumasun_td.time_evo_H4.h, which brings in the QUMASUN_TD class). */
+#include "poisson_fft.h"
+#include "Vxc.h"
+#include "SetOccupancy.h"
+#include "GridGradient8th.h"
+#include "qumasun_td.time_evo_H4.h"
+
 namespace {
 
 struct NullWatch {
@@ -425,6 +435,17 @@ struct RefKpointHamiltonian {
                 }
             }
         }
+#ifdef EXPAND_PROJECTOR_YLM_Z
+        /* UpdateNonlocalBlock also expanded projector * Y_lm into projector_RY_expikx (the
+         * table the force inner products read, mInnerNonlocalPsi_b3*) while the radial part
+         * was still 1: expand again now that projector_expikx carries w_k. */
+        for (int a = 0; a < d->n_atoms; ++a) {
+            auto& proj = pp.m_nonlocal_projectors[a];
+            for (auto* b : proj.projector_RY_expikx) delete[] b;
+            proj.projector_RY_expikx.clear();
+            pp.mExpandProjectorYlm(pp.m_nonlocal_blocks[a], proj, 0);
+        }
+#endif
     }
 
     /* One {re, im} state, in the order of mHamiltonianMatrix_ddm (qumasun_kpoint.matrix.h:25-50). */
@@ -495,6 +516,110 @@ int ref_lobpcg_z_multi(const ref_ham_desc* d, double gx, double gy, double gz, d
                                   (OneComplex*)nullptr, 0, 0, OpeA, watch);
     }
     if (iters) *iters = (int)((calls - 2LL * ns) / ns);
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* V_tot = V_ext + V_hart + V_x + V_c as QUMASUN_SINGLE::mSetPotential forms it for
+ * KohnSham_PP without spin (qumasun_single.potential.h:33-43): V_hart by
+ * SetPotentialByPoissonFFT (poisson_fft.h:14-128, the free-function form of
+ * mSetPotentialVhart, :101-200), V_x and V_c by Calc_XC_LDA(rho + pcc) per point
+ * (mSetPotentialVxc, :311-317; Vxc.h:41-70). pcc may be NULL (zero). */
+int ref_potential_lda(int nx, int ny, int nz, double hx, double hy, double hz, const double* rho, const double* pcc,
+                      const double* vext, double* vtot, double* vhart, double* vx, double* vc) {
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<double> work(N * 4);
+    SetPotentialByPoissonFFT(vhart, rho, nx, ny, nz, hx, hy, hz, work.data());
+    for (size_t i = 0; i < N; ++i) {
+        const Return_XC r = Calc_XC_LDA(rho[i] + (pcc ? pcc[i] : 0.0));
+        vx[i] = r.V_x;
+        vc[i] = r.V_c;
+    }
+    for (size_t i = 0; i < N; ++i) vtot[i] = vext[i] + vhart[i] + vx[i] + vc[i];
+    return 0;
+}
+
+/* Fermi occupations at a given chemical potential (SetOccupancy.h:7-18); returns the sum. */
+double ref_set_occupancy(double coef, double kbT, int n, const double* ev, double mu, double* occ) {
+    return SetOccupancy(coef, kbT, n, ev, mu, occ);
+}
+
+/* out_{x,y,z} = coef * grad psi, 8th order, periodic (Gradient8th, GridGradient8th.h:219-235). */
+int ref_gradient8(int nx, int ny, int nz, double hx, double hy, double hz, double coef, const double* psi,
+                  double* gx_out, double* gy_out, double* gz_out) {
+    GridRange grid{0, 0, 0, nx, ny, nz};
+    Gradient8th(grid, gx_out, gy_out, gz_out, psi, coef, hx, hy, hz);
+    return 0;
+}
+
+/* One Taylor-4 step of ns complex states ({re, im} per state, X[s*2N ..]) with the
+ * reference k-point H at Bloch vector g: QUMASUN::TimeEvoH4 (qumasun_td.time_evo_H4.h:13-60)
+ * run unchanged on one rank. */
+int ref_td_taylor4(const ref_ham_desc* d, double gx, double gy, double gz, double rc, double dt, int ns,
+                   double* X) {
+    if (d->fd_order != 8) return -1;
+    RefKpointHamiltonian H(d, gx, gy, gz, rc);
+    if (H.status) return H.status;
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    const double dV = d->hx * d->hy * d->hz;
+    std::vector<SoAComplex> xs(ns);
+    for (int s = 0; s < ns; ++s) {
+        xs[s].re = X + (size_t)s * 2 * N;
+        xs[s].im = X + (size_t)s * 2 * N + N;
+    }
+    auto OpeA = [&](SoAComplex& Ax, const SoAComplex& x) { H.Apply(Ax.re, Ax.im, x.re, x.im); };
+    NullWatch watch;
+    QUMASUN::TimeEvoH4(H.grid, dV, dt, ns, xs.data(), OpeA, watch);
+    return 0;
+}
+
+/* Nonlocal energy and forces of ns complex states at Bloch vector g, as
+ * QUMASUN_KPOINT::mGetForcePseudoNonlocal forms them (qumasun_kpoint.force.h:238-258):
+ * for each state with occ > 0, dpsi = -2 occ grad psi (Gradient8th on re and im) and
+ * PseudoPotIntegrator_kpoint::ForceNonlocal (PseudoPotOperator_kpoint_v2.h:2760-2866)
+ * with g scaled by -2 occ. forces (3 per atom) accumulate; e_state[s] receives the
+ * state's nonlocal energy (0 for occ <= 0); *ev_sum = sum_s occ_s e_state[s].
+ * At g = 0 with zero imaginary parts this is the Gamma-point real-state force of
+ * QUMASUN_MPI::mGetForcePseudoNonlocal (qumasun_mpi.force.h:227-254). */
+int ref_nonlocal_force_z(const ref_ham_desc* d, double gx, double gy, double gz, double rc, int ns,
+                         const double* X, const double* occ, double* forces, double* e_state, double* ev_sum) {
+    if (d->fd_order != 8) return -1;
+    RefKpointHamiltonian H(d, gx, gy, gz, rc);
+    if (H.status) return H.status;
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    std::vector<double> buf(6 * N);
+    SoAComplex dx{buf.data(), buf.data() + N}, dy{buf.data() + 2 * N, buf.data() + 3 * N},
+        dz{buf.data() + 4 * N, buf.data() + 5 * N};
+    GridRange grid{0, 0, 0, d->nx, d->ny, d->nz};
+    double ev = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        e_state[s] = 0.0;
+        if (occ[s] <= 0.0) continue;
+        const double coef = -2.0 * occ[s];
+        SoAComplex psi{const_cast<double*>(X + (size_t)s * 2 * N), const_cast<double*>(X + (size_t)s * 2 * N + N)};
+        Gradient8th(grid, dx.re, dy.re, dz.re, psi.re, coef, d->hx, d->hy, d->hz);
+        Gradient8th(grid, dx.im, dy.im, dz.im, psi.im, coef, d->hx, d->hy, d->hz);
+        const double e = H.pp.ForceNonlocal(forces, psi, dx, dy, dz, H.grid, H.nuclei.data(), d->n_atoms, 0,
+                                            gx * coef, gy * coef, gz * coef);
+        e_state[s] = e;
+        ev += e * occ[s];
+    }
+    if (ev_sum) *ev_sum = ev;
+    return 0;
+}
+
+/* Nonlocal energy of each real state (PseudoPotIntegrator_single::EnergyPPnonlocal,
+ * PseudoPotOperator.h:775-816), X state-major (ns * N). */
+int ref_nonlocal_energy_d(const ref_ham_desc* d, int ns, const double* X, double* e_state) {
+    RefHamiltonian H(d);
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    for (int s = 0; s < ns; ++s) {
+        RspaceFunc<double> psi(const_cast<double*>(X + (size_t)s * N));
+        e_state[s] = H.pp.EnergyPPnonlocal(psi, H.nuclei.data(), d->n_atoms);
+    }
     return 0;
 }
 

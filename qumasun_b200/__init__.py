@@ -6,6 +6,8 @@ The compute path is the C ABI of ``include/qumasun_b200.h`` implemented in
 * :mod:`qumasun_b200.cell`   -- synthetic diamond cells, analytic V and projector tables;
 * :mod:`qumasun_b200.engine` -- Context / Hamiltonian over the shared library.
 """
-from .engine import Context, Hamiltonian, LearnedPreconditioner, QGError, lib  # noqa: F401
+from .engine import (Context, Hamiltonian, LearnedPreconditioner, Poisson, QGError, density,  # noqa: F401
+                     lib, occupancy)
 
-__all__ = ["Context", "Hamiltonian", "LearnedPreconditioner", "QGError", "lib"]
+__all__ = ["Context", "Hamiltonian", "LearnedPreconditioner", "Poisson", "QGError", "density", "lib",
+           "occupancy"]

@@ -74,6 +74,8 @@ int qg_context_destroy(qg_context c) {
     cudaSetDevice(c->device);
     qg_release_libraries(c);
     qg_release_gram_cache(c);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->small.release();
     if (c->own_stream) {
         cudaStreamSynchronize(c->own_stream);
         cudaStreamDestroy(c->own_stream);

@@ -386,7 +386,7 @@ constexpr int kProjDepth = 3;  // cp.async stages of the projection's gather
 
 template <typename T, int NCH>
 static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, const T* X, long long ldx, T* coef,
-                              long long ldc, int sb, int parts, cudaStream_t st) {
+                              long long ldc, int sb, int parts, cudaStream_t st, const double* scale) {
     // register budget: 16 states only with 4 channels, 8 with 8, 4 with 16
     constexpr int kMaxSb = NCH <= 4 ? 16 : (NCH == 8 ? 8 : 4);
     sb = std::min(sb, kMaxSb);
@@ -399,7 +399,7 @@ static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, con
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) \
             return QG_ERR_CUDA;                                                                                \
         e = launch_clustered(kern, g, dim3(kProjThreads), parts, smem, st, X, ldx, ns, pj.atom_off, pj.pt_g,   \
-                             tab, pj.npts, pj.ch_scale, coef, ldc, parts);                                     \
+                             tab, pj.npts, scale, coef, ldc, parts);                                           \
     } while (0)
     switch (sb) {
         case 16:
@@ -423,20 +423,27 @@ static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, con
     return QG_OK;
 }
 
+// scale[atom * nch + ch] multiplies each sum (nullptr: E_k * dV, the operator's coefficients).
 template <typename T>
 static int launch_project(const DevProjectors& pj, int ns, const T* X, long long ldx, T* coef, long long ldc,
-                          int forced_sb, int forced_parts, cudaStream_t st) {
+                          int forced_sb, int forced_parts, cudaStream_t st, const double* scale = nullptr) {
     const T* tab;
     if constexpr (sizeof(T) == 8) tab = reinterpret_cast<const T*>(pj.tab_d);
     else tab = reinterpret_cast<const T*>(pj.tab_f);
+    if (!scale) scale = pj.ch_scale;
     const int parts = project_parts(pj, forced_parts);
     const int sb = pick_project_sb(pj.na * parts, ns, forced_sb);
     switch (pj.nch) {
-        case 4: return launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
-        case 8: return launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
-        case 16: return launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st);
+        case 4: return launch_project_nch<T, 4>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st, scale);
+        case 8: return launch_project_nch<T, 8>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st, scale);
+        case 16: return launch_project_nch<T, 16>(pj, tab, ns, X, ldx, coef, ldc, sb, parts, st, scale);
         default: return QG_ERR_UNSUPPORTED;
     }
+}
+
+int project_inner_d(qg_hamiltonian h, int ns, const double* X, long long ldx, double* coef, long long ldc,
+                    cudaStream_t st) {
+    return launch_project<double>(h->pj, ns, X, ldx, coef, ldc, h->proj_sb, h->proj_parts, st, h->pj.ch_dv);
 }
 
 // 16-byte vector of T (the unit the scatter reads the coefficients in).
@@ -595,6 +602,23 @@ size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk) {
     return (size_t)2 * nk * coef_ld(nsk) * pj.na * pj.nch;
 }
 
+// Stencil kernel for a real-state apply: the forced variant when it accepts the shape,
+// else the one-plane ring kernel (measured faster than the two-plane one on the 80^3
+// cell at every order: 0.76 against 0.90 ms at order 8), else the two-plane ring
+// kernel, else (1) the register-window kernel, which takes any shape.
+template <typename T>
+static int ring_stencil_variant(qg_hamiltonian h, const HamArgs<T>& a) {
+    const int v = h->stencil_variant;
+    if (v == 1) return 1;
+    const bool pair_ok = stencil_pair_ok<T>(a, h->order);
+    const bool tma_ok = stencil_tma_ok<T>(a, h->order);
+    if (v == 3 && pair_ok) return 3;
+    if (v == 2 && tma_ok) return 2;
+    if (tma_ok) return 2;
+    if (pair_ok) return 3;
+    return 1;
+}
+
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
                       T* coef, cudaStream_t st, PhaseTimer* pt) {
@@ -645,10 +669,14 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
     a.err = h->ctx->dev_status;
     const bool nonlocal = pj.na > 0 && pj.nch > 0;
     const long long N = h->N();
-    if (!h->force_plain_stencil && stencil_tma_ok<T>(a, h->order)) {
+    const int variant = ring_stencil_variant<T>(h, a);
+    if (variant != 1) {
+        auto stencil = [&]() {
+            return variant == 3 ? launch_stencil_pair<T>(a, h->order, st) : launch_stencil_tma<T>(a, h->order, st);
+        };
         if (!nonlocal) {
             if (pt) pt->mark(1, st);
-            QG_TRY(launch_stencil_tma<T>(a, h->order, st));
+            QG_TRY(stencil());
             QG_CUDA_TRY(cudaGetLastError());
             if (pt) pt->mark(-1, st);
             return QG_OK;
@@ -657,7 +685,7 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
         if (pt) pt->mark(0, st);
         QG_TRY(launch_project<T>(pj, ns, X, ldx, coef, coef_ld(ns), h->proj_sb, h->proj_parts, st));
         if (pt) pt->mark(1, st);
-        QG_TRY(launch_stencil_tma<T>(a, h->order, st));
+        QG_TRY(stencil());
         if (pt) pt->mark(2, st);
         QG_TRY(launch_scatter_all<T>(pj, HX, ldhx, ns, N, coef, coef_ld(ns), h->scatter_sg, st));
         if (pt) pt->mark(-1, st);
@@ -718,7 +746,7 @@ int upload(T** dst, const std::vector<T>& src) {
 
 void free_projectors(DevProjectors& pj) {
     cudaFree(pj.atom_off); cudaFree(pj.pt_g); cudaFree(pj.tab_d); cudaFree(pj.tab_f);
-    cudaFree(pj.ch_scale); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
+    cudaFree(pj.ch_scale); cudaFree(pj.ch_dv); cudaFree(pj.ch_E); cudaFree(pj.row); cudaFree(pj.ent_atom); cudaFree(pj.ent_val_d);
     cudaFree(pj.ent_val_f); cudaFree(pj.pt_u); cudaFree(pj.ent_pt); cudaFree(pj.ztab); cudaFree(pj.zent);
     cudaFree(pj.ztab_f); cudaFree(pj.zent_f);
     pj = DevProjectors();
@@ -746,7 +774,7 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
     std::vector<int> atom_off(na + 1, 0);
     std::vector<int> pt_g, pt_u;
     std::vector<std::vector<double>> tabs(nch);
-    std::vector<double> ch_scale((size_t)na * nch, 0.0);
+    std::vector<double> ch_scale((size_t)na * nch, 0.0), ch_dv((size_t)na * nch, 0.0), ch_E((size_t)na * nch, 0.0);
     std::vector<int> ch_k(nch, -1), ch_m(nch, 0);
     {
         int c = 0;
@@ -763,8 +791,11 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
                 hi[i] = std::max(hi[i], c[i] + c[3 + i]);
             }
         }
-        for (int ch = 0; ch < nch; ++ch)
+        for (int ch = 0; ch < nch; ++ch) {
             ch_scale[(size_t)a * nch + ch] = ch_k[ch] >= 0 ? d->proj_E[ch_k[ch]] * dV : 0.0;
+            ch_dv[(size_t)a * nch + ch] = ch_k[ch] >= 0 ? dV : 0.0;
+            ch_E[(size_t)a * nch + ch] = ch_k[ch] >= 0 ? d->proj_E[ch_k[ch]] : 0.0;
+        }
         std::vector<double> vals(nch);
         for (int z = lo[2]; z < hi[2]; ++z)
             for (int y = lo[1]; y < hi[1]; ++y)
@@ -827,6 +858,8 @@ int build_projectors(qg_hamiltonian h, const qg_hamiltonian_desc* d) {
     QG_TRY(upload(&pj.tab_d, tab_d));
     QG_TRY(upload(&pj.tab_f, tab_f));
     QG_TRY(upload(&pj.ch_scale, ch_scale));
+    QG_TRY(upload(&pj.ch_dv, ch_dv));
+    QG_TRY(upload(&pj.ch_E, ch_E));
     QG_TRY(upload(&pj.row, row));
     QG_TRY(upload(&pj.ent_atom, ent_atom));
     QG_TRY(upload(&pj.ent_val_d, ent_val));
@@ -844,6 +877,7 @@ void destroy_ham(qg_hamiltonian h) {
     free_projectors(h->pj);
     h->coef.release();
     h->kco.release();
+    h->scf_work.release();
     if (h->io_in) cudaStreamDestroy(h->io_in);
     if (h->io_out) cudaStreamDestroy(h->io_out);
     h->xio.release();
@@ -1019,9 +1053,9 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long
     return QG_OK;
 }
 
-int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int plain) {
-    if (!h || (plain != 0 && plain != 1)) return QG_ERR_INVALID;
-    h->force_plain_stencil = plain;
+int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int variant) {
+    if (!h || variant < 0 || variant > 3) return QG_ERR_INVALID;
+    h->stencil_variant = variant;
     return QG_OK;
 }
 
@@ -1046,7 +1080,7 @@ int qg_hamiltonian_launches_per_apply(qg_hamiltonian h, int ns) {
     qg::HamArgs<double> a{};
     a.X = reinterpret_cast<const double*>(16); a.HX = reinterpret_cast<double*>(16); a.V = h->V_d;
     a.ldx = a.ldhx = h->N(); a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.err = h->ctx->dev_status;
-    if (!h->force_plain_stencil && qg::stencil_tma_ok<double>(a, h->order)) {
+    if (qg::ring_stencil_variant<double>(h, a) != 1) {
         if (!nonlocal) return 1;
         return 3;  // projection, stencil + V, nonlocal scatter
     }

@@ -467,7 +467,7 @@ int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, co
     }
     if (pt) pt->mark(1, st);
     constexpr int PX = 16 / sizeof(T);
-    if (h->force_plain_stencil || !stencil_tma_ok<T>(a, 8, 2) || (nk > 1 && (ldk % PX || ldkh % PX))) {
+    if (h->stencil_variant == 1 || !stencil_tma_ok<T>(a, 8, 2) || (nk > 1 && (ldk % PX || ldkh % PX))) {
         dim3 g((unsigned)((N + 255) / 256), (unsigned)(nk * nsk));
         k_kpoint_plain<T><<<g, 256, 0, st>>>(a);
     } else {

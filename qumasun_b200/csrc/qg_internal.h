@@ -26,20 +26,6 @@
 
 void qg_set_last_error(const char* what, const char* msg, const char* file, int line);
 
-struct qg_context_s {
-    int device = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    void* blas = nullptr;      // cublasHandle_t, created on first use
-    void* solver = nullptr;    // cusolverDnHandle_t, created on first use
-    int live_hamiltonians = 0; // the context outlives every operator built on it
-    int* dev_status = nullptr; // device status word set by kernels whose bounded waits gave up
-    void* gram_cache = nullptr; // qg::MixedGram buffers kept by qg_gram_mixed_d across calls
-};
-
-// Frees the context's qg_gram_mixed_d buffers (gram_mixed.cu).
-void qg_release_gram_cache(qg_context c);
-
 // A device buffer that only grows.
 struct DevBuf {
     void* ptr = nullptr;
@@ -61,6 +47,21 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+struct qg_context_s {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    void* blas = nullptr;      // cublasHandle_t, created on first use
+    void* solver = nullptr;    // cusolverDnHandle_t, created on first use
+    int live_hamiltonians = 0; // the context outlives every operator built on it
+    int* dev_status = nullptr; // device status word set by kernels whose bounded waits gave up
+    void* gram_cache = nullptr; // qg::MixedGram buffers kept by qg_gram_mixed_d across calls
+    DevBuf small;               // per-call state lists of the density entry points
+};
+
+// Frees the context's qg_gram_mixed_d buffers (gram_mixed.cu).
+void qg_release_gram_cache(qg_context c);
+
 // Nonlocal projector tables on the device, in two orders:
 //  gather side (atom-major): atom a owns points [atom_off[a], atom_off[a+1]) of
 //    pt_g (grid index) and tab[ch*npts + p] (channel values w*Y);
@@ -76,6 +77,8 @@ struct DevProjectors {
     double* tab_d = nullptr;
     float* tab_f = nullptr;
     double* ch_scale = nullptr;  // E_k * dV per (atom, channel)
+    double* ch_dv = nullptr;     // dV per (atom, channel) with a projector (0 for padding channels)
+    double* ch_E = nullptr;      // E_k per (atom, channel) (0 for padding channels)
     int* row = nullptr;
     int* ent_atom = nullptr;
     double* ent_val_d = nullptr;
@@ -117,9 +120,12 @@ struct qg_hamiltonian_s {
     DevBuf coef;      // projector coefficients E*dV*<p|psi>, [ns][na*nch]
     DevBuf xio, hxio; // staging for the host-buffer entry point
     DevBuf kco;       // per-k-point stencil coefficients of a multi-k apply
+    DevBuf scf_work;  // propagation blocks, gradients and inner products (scf.cu)
     cudaStream_t io_in = nullptr, io_out = nullptr;  // copy streams of the host-buffer entry points
     int ty = 1;       // grid rows per stencil tile
-    int force_plain_stencil = 0;  // 1: always use the register-window stencil kernel
+    // stencil kernel of the real-state apply: 0 = engine's choice, 1 = register-window
+    // kernel (any shape), 2 = one-plane TMA ring, 3 = two-plane TMA ring
+    int stencil_variant = 0;
     int proj_sb = 0;     // states per projection block (0: chosen per launch)
     int proj_parts = 0;  // blocks (one cluster) per atom in the projection (0: from the cell)
     int scatter_sg = 0;  // states per scatter group (0: 8)
@@ -218,6 +224,11 @@ size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk);
 template <typename T>
 int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long long ldhx,
                       T* coef_scratch, cudaStream_t st, PhaseTimer* pt = nullptr);
+
+// Inner products dV <p_{a,ch}|psi_s> of ns real states, channel-major like the
+// operator's coefficients: coef[(a * nch + ch) * ldc + s] (hamiltonian.cu).
+int project_inner_d(qg_hamiltonian h, int ns, const double* X, long long ldx, double* coef, long long ldc,
+                    cudaStream_t st);
 
 // Complex k-point H (kpoint.cu): state s has its real part at X + s*ldx and its
 // imaginary part N elements later; coef_scratch holds 2*coef_scratch_elems(h, ns) doubles.

@@ -59,5 +59,10 @@ int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc =
 // True when launch_stencil_tma accepts this shape and alignment.
 template <typename T>
 bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc = 1);
+// Real states, two output planes per consumer step (stencil_pair.cu).
+template <typename T>
+int launch_stencil_pair(const HamArgs<T>& a, int order, cudaStream_t st);
+template <typename T>
+bool stencil_pair_ok(const HamArgs<T>& a, int order);
 
 }  // namespace qg

@@ -442,6 +442,8 @@ int ring_stages_for(int R, size_t stage_bytes) {
     return nst >= need ? nst : -1;
 }
 
+}  // namespace
+
 // SM count of the current device, looked up once per device (devices of one process
 // may differ: MIG slices, mixed parts). Racing first lookups store the same value.
 int sm_count() {
@@ -458,6 +460,8 @@ int sm_count() {
     cache[dev].store(n, std::memory_order_relaxed);
     return n;
 }
+
+namespace {
 
 template <typename T, int ORDER, int NC, int NXC = 0>
 int launch_order(const HamArgs<T>& a, cudaStream_t st) {

@@ -149,6 +149,16 @@ def lib():
         L.qg_lobpcg_cells_device.argtypes = [C.c_int, C.POINTER(vp), C.POINTER(LobpcgOptions), _ip,
                                              C.POINTER(_dp), C.POINTER(vp), C.POINTER(vp),
                                              C.POINTER(LobpcgReport), _ip]
+        L.qg_density_d.argtypes = [vp, C.c_longlong, C.c_int, vp, C.c_longlong, _dp, vp, C.c_int]
+        L.qg_density_z.argtypes = [vp, C.c_longlong, C.c_int, vp, C.c_longlong, _dp, vp, C.c_int]
+        L.qg_occupancy.argtypes = [C.c_double, C.c_int, _dp, C.c_int, _dp, _dp]
+        L.qg_occupancy_spin.argtypes = [C.c_double, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _dp]
+        L.qg_poisson_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        C.POINTER(vp)]
+        L.qg_poisson_destroy.argtypes = [vp]
+        L.qg_potential_lda_d.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+        L.qg_td_taylor4_z.argtypes = [vp, C.c_int, C.c_double, vp, C.c_longlong]
+        L.qg_nonlocal_force_d.argtypes = [vp, C.c_int, vp, C.c_longlong, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -199,6 +209,77 @@ class Context:
 
 def _ptr(a, t):
     return a.ctypes.data_as(t)
+
+
+def _dev(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def density(ctx, X, occ, rho=None, accumulate=False, complex_states=False):
+    """rho (+)= sum_s occ[s] |psi_s|^2 on the device (qg_density_d / _z): X a CUDA float64
+    tensor (ns, N) of real states or (ns, 2N) of {re, im} states, occ host values."""
+    import torch
+    occ = np.ascontiguousarray(occ, dtype=np.float64)
+    ns = X.shape[0]
+    N = X.shape[1] // (2 if complex_states else 1)
+    if occ.shape[0] != ns:
+        raise ValueError("one occupation per state")
+    if not (X.is_cuda and X.dtype == torch.float64 and X.is_contiguous()):
+        raise TypeError("X must be a contiguous float64 CUDA tensor")
+    if rho is None:
+        rho = torch.zeros(N, dtype=torch.float64, device=X.device)
+        accumulate = False
+    ctx.use_torch_stream()
+    fn = lib().qg_density_z if complex_states else lib().qg_density_d
+    check(fn(ctx.h, N, ns, _dev(X), X.shape[1], occ.ctypes.data_as(_dp), _dev(rho), 1 if accumulate else 0),
+          "qg_density")
+    return rho
+
+
+def occupancy(kbT, ev, n_electrons, ev_down=None):
+    """Fermi occupations by bisection on mu (qg_occupancy / qg_occupancy_spin).
+    Returns (occ, mu) or ((occ_up, occ_down), mu) with ev_down."""
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    mu = C.c_double()
+    if ev_down is None:
+        occ = np.zeros_like(ev)
+        check(lib().qg_occupancy(kbT, len(ev), ev.ctypes.data_as(_dp), int(n_electrons), occ.ctypes.data_as(_dp),
+                                 C.byref(mu)), "qg_occupancy")
+        return occ, mu.value
+    ed = np.ascontiguousarray(ev_down, dtype=np.float64)
+    ou, od = np.zeros_like(ev), np.zeros_like(ed)
+    check(lib().qg_occupancy_spin(kbT, len(ev), ev.ctypes.data_as(_dp), ed.ctypes.data_as(_dp), int(n_electrons),
+                                  ou.ctypes.data_as(_dp), od.ctypes.data_as(_dp), C.byref(mu)), "qg_occupancy_spin")
+    return (ou, od), mu.value
+
+
+class Poisson:
+    """FFT Poisson + LDA potential builder of one periodic grid (qg_poisson)."""
+
+    def __init__(self, ctx: Context, grid, h):
+        self.ctx = ctx
+        self.N = int(grid[0] * grid[1] * grid[2])
+        self.h = C.c_void_p()
+        check(lib().qg_poisson_create(ctx.h, int(grid[0]), int(grid[1]), int(grid[2]), float(h[0]), float(h[1]),
+                                      float(h[2]), C.byref(self.h)), "qg_poisson_create")
+        self._fin = weakref.finalize(self, lib().qg_poisson_destroy, self.h)
+
+    def potential(self, rho, vext, pcc=None, parts=False):
+        """V_tot (and with parts=True also V_hart, V_x, V_c) from CUDA float64 tensors of N values."""
+        import torch
+        for t, n in ((rho, "rho"), (vext, "vext"), (pcc, "pcc")):
+            if t is not None and not (t.is_cuda and t.dtype == torch.float64 and t.numel() == self.N
+                                      and t.is_contiguous()):
+                raise TypeError(f"{n} must be a contiguous float64 CUDA tensor of {self.N} values")
+        out = [torch.empty_like(rho) for _ in range(4 if parts else 1)]
+        extra = [_dev(o) for o in out[1:]] + [None] * (3 - len(out[1:]))
+        self.ctx.use_torch_stream()
+        check(lib().qg_potential_lda_d(self.h, _dev(rho), _dev(pcc), _dev(vext), _dev(out[0]), *extra),
+              "qg_potential_lda_d")
+        return tuple(out) if parts else out[0]
+
+    def close(self):
+        self._fin()
 
 
 def sygv_small_batched(ctx, A, B):
@@ -513,6 +594,31 @@ class Hamiltonian:
         return tuple(ph)
 
     # ---- complex k-point operator: states are (ns, 2N) rows {re[N], im[N]}
+    def td_taylor4(self, X, dt):
+        """One Taylor-4 propagation step of {re, im} states X (CUDA float64 (ns, 2N), in place)."""
+        import torch
+        if not (X.is_cuda and X.dtype == torch.float64 and X.is_contiguous() and X.dim() == 2
+                and X.shape[1] == 2 * self.N):
+            raise TypeError(f"X must be a contiguous float64 CUDA tensor (ns, {2 * self.N})")
+        self.ctx.use_torch_stream()
+        check(lib().qg_td_taylor4_z(self.h, X.shape[0], float(dt), _dev(X), X.shape[1]), "qg_td_taylor4_z")
+        return X
+
+    def nonlocal_force(self, X, occ, forces=None):
+        """(forces (na, 3), e_state (ns,), EV) of real states X (CUDA float64 (ns, N))."""
+        import torch
+        self._check_block(X, "X", (torch.float64,))
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        na = self.cell.n_atoms if len(self.cell.proj_l) else 0
+        f = np.zeros(3 * na) if forces is None else np.ascontiguousarray(forces, dtype=np.float64).reshape(-1).copy()
+        e = np.zeros(X.shape[0])
+        ev = C.c_double()
+        self.ctx.use_torch_stream()
+        check(lib().qg_nonlocal_force_d(self.h, X.shape[0], _dev(X), X.shape[1], occ.ctypes.data_as(_dp),
+                                        f.ctypes.data_as(_dp), e.ctypes.data_as(_dp), C.byref(ev)),
+              "qg_nonlocal_force_d")
+        return f.reshape(na, 3), e, ev.value
+
     def set_kvector(self, g):
         check(lib().qg_hamiltonian_set_kvector(self.h, float(g[0]), float(g[1]), float(g[2])),
               "qg_hamiltonian_set_kvector")
@@ -580,9 +686,11 @@ class Hamiltonian:
         check(lib().qg_hamiltonian_set_learned(self.h, nn.h if nn is not None else None, float(vscale)),
               "qg_hamiltonian_set_learned")
 
-    def set_stencil_kernel(self, plain: bool):
-        """False: TMA-staged ring kernel where the shape allows (default); True: register-window kernel."""
-        check(lib().qg_hamiltonian_set_stencil_kernel(self.h, 1 if plain else 0), "qg_hamiltonian_set_stencil_kernel")
+    def set_stencil_kernel(self, variant):
+        """Stencil kernel of the real-state apply: 0 (or False) = engine's choice, 1 (or
+        True) = register-window kernel, 2 = one-plane TMA ring, 3 = two-plane TMA ring."""
+        v = int(variant)
+        check(lib().qg_hamiltonian_set_stencil_kernel(self.h, v), "qg_hamiltonian_set_stencil_kernel")
 
     def set_nonlocal_blocking(self, project_states=0, scatter_states=0, project_parts=0):
         """States per projection block (1/2/4/8/16), per scatter group (4/8) and blocks per

@@ -6,7 +6,11 @@ Every array comes from the reference functions driven by oracle/ref_harness.cpp:
 Laplasian{2,4,6,8}th_halo, LaplasianKpoint8th_halo, the reference Hamiltonian
 (V, ProjectionPP, kinetic), the reference k-point Hamiltonian (V,
 PseudoPotIntegrator_kpoint::ProjectionPP, LaplasianKpoint8th; `--kpoint` writes
-only ham_kpoint.npz) and GridForSphere / SetYlmAround tables.
+only ham_kpoint.npz) and GridForSphere / SetYlmAround tables. `--scf` writes
+scf.npz: the FFT Poisson + LDA potential (SetPotentialByPoissonFFT, Calc_XC_LDA),
+Fermi occupations (SetOccupancy), the 8th-order gradient (Gradient8th), one Taylor-4
+step (QUMASUN::TimeEvoH4) and nonlocal energies and forces
+(PseudoPotIntegrator_kpoint::ForceNonlocal, PseudoPotIntegrator_single::EnergyPPnonlocal).
 """
 import os
 import sys
@@ -151,7 +155,40 @@ def make_lobpcg_kpoint():
     print("wrote lobpcg_kpoint", out["small_ev"], out["d8_ev"])
 
 
-if __name__ == "__main__" and "--lobpcg-kpoint" in sys.argv:
+def make_scf():
+    """Reference outputs of the SCF-step neighbours on the non-cubic 20x16x24 cell."""
+    cell = build_cell(grid=(20, 16, 24))
+    grid = (cell.nx, cell.ny, cell.nz)
+    h = (cell.hx, cell.hy, cell.hz)
+    X = initial_states(3, cell.N, seed=41)
+    occ = np.array([2.0, 1.5, 0.0])
+    rng = np.random.default_rng(42)
+    # a density spanning both LDA branches (rs < 1 and rs >= 1) and the 1e-8 cut-off
+    rho = 0.6 * O.density(X, occ)
+    rho[::97] = 0.0
+    pcc = 0.05 * np.exp(-((np.arange(cell.N) % 37) / 9.0) ** 2)
+    vt, vh, vx, vc = O.potential_lda(grid, h, rho, cell.V, pcc=pcc, impl="ref")
+    ev = np.sort(rng.uniform(-0.9, 0.4, 24))
+    occ_mu, tot_mu = O.fermi(2.0, 0.01, ev, -0.2, impl="ref")
+    occ_b, mu_b = O.occupancy(0.01, ev, 30, impl="ref")
+    gx, gy, gz = O.gradient8(grid, h, -3.0, X[0], impl="ref")
+    Z = np.ascontiguousarray(np.concatenate([X[:2], 0.4 * X[1:3][::-1]], axis=1))
+    g = (0.31, -0.17, 0.05)
+    Zt = O.td_taylor4(cell, g, 0.02, Z, impl="ref")
+    f_r, e_r, ev_r = O.nonlocal_force(cell, X, occ, impl="ref")
+    f_z, e_z, ev_z = O.nonlocal_force(cell, Z, occ[:2], g=g, impl="ref")
+    e_single = O.nonlocal_energy(cell, X)
+    np.savez_compressed(os.path.join(HERE, "scf.npz"), grid=np.array(grid), h=np.array(h), X=X, occ=occ,
+                        rho=rho, pcc=pcc, vtot=vt, vhart=vh, vx=vx, vc=vc, ev=ev, occ_mu=occ_mu, tot_mu=tot_mu,
+                        occ_bisect=occ_b, mu_bisect=mu_b, grad=np.stack([gx, gy, gz]), Z=Z, g=np.array(g),
+                        dt=0.02, Z_taylor4=Zt, force_real=f_r, e_real=e_r, ev_real=ev_r, force_z=f_z, e_z=e_z,
+                        ev_z=ev_z, e_single=e_single)
+    print("wrote scf", ev_r, ev_z, mu_b)
+
+
+if __name__ == "__main__" and "--scf" in sys.argv:
+    make_scf()
+elif __name__ == "__main__" and "--lobpcg-kpoint" in sys.argv:
     make_lobpcg_kpoint()
 elif __name__ == "__main__" and "--kpoint" in sys.argv:
     make_kpoint()
