@@ -241,7 +241,11 @@ typedef struct qg_lobpcg_report {
  * Jacobi-equilibrated (scaled to unit diag(B)) and solved with cuSOLVER's
  * sygvd; if B is still not positive definite, the step is solved on the span
  * of B's eigenvectors with eigenvalues above 1e-12 max (counted in
- * report->restarts) instead of stopping. Returns QG_ERR_NOT_CONVERGED (results
+ * report->restarts) instead of stopping. A rotated Ritz vector whose |x|^2 dV drifts
+ * from 1 by more than 1e-3 rolls the step back (the check of Eigen_d_multi_mpi,
+ * lobpcg_d_multi_mpi.h:1305-1346): X and P are kept, the next step solves the [x r]
+ * pencil from a full Gram (counted in report->restarts; 20 rollbacks end the solve with
+ * QG_ERR_CHOLESKY). Returns QG_ERR_NOT_CONVERGED (results
  * still written) when max_iter is reached, QG_ERR_CHOLESKY if fewer than ns
  * independent directions remain. */
 int qg_lobpcg_d(qg_hamiltonian ham, const qg_lobpcg_options* opt, int ns, double* ev, double* X,
@@ -378,6 +382,20 @@ int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int variant);
  * bits only), and the engine's choice never depends on the number of states. */
 int qg_hamiltonian_set_nonlocal_blocking(qg_hamiltonian ham, int project_states, int scatter_states,
                                          int project_parts);
+/* Real-state LOBPCG (qg_lobpcg_d, _device, cells) with more than 128 Gram columns: 1
+ * (default) forms the steady-state pencil from the previous rotation -- only the blocks
+ * with the new residuals are tall products ([x r p]^T A r, [x r p]^T r), the x/p blocks
+ * are Z^T S Z of the last pencil (the direct update of NextMatrix_d,
+ * lobpcg_d_multi_mpi.h:264-460) -- with a full Gram every 10 iterations and after any
+ * 2n step, rank-revealing solve or rollback; 0 forms the full Gram every iteration. */
+int qg_hamiltonian_set_gram_reuse(qg_hamiltonian ham, int on);
+/* Test hook of the bounded waits: with on = 1 the producer lane of the ring stencil
+ * kernels (real states) issues no copy, so every consumer's bounded mbarrier wait
+ * (about 2^31 SM clocks) runs out; the kernels then wind down, record QG_ERR_TIMEOUT
+ * in the context's device status word (qg_context_synchronize /
+ * qg_context_take_device_status) and the context stays usable. 0 restores normal
+ * operation. Nothing in the library sets it. */
+int qg_hamiltonian_test_stall(qg_hamiltonian ham, int on);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
 

@@ -667,6 +667,7 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
         default: return QG_ERR_INVALID;
     }
     a.err = h->ctx->dev_status;
+    a.stall = h->test_stall;
     const bool nonlocal = pj.na > 0 && pj.nch > 0;
     const long long N = h->N();
     const int variant = ring_stencil_variant<T>(h, a);
@@ -1056,6 +1057,12 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int variant) {
     if (!h || variant < 0 || variant > 3) return QG_ERR_INVALID;
     h->stencil_variant = variant;
+    return QG_OK;
+}
+
+int qg_hamiltonian_test_stall(qg_hamiltonian h, int on) {
+    if (!h || (on != 0 && on != 1)) return QG_ERR_INVALID;
+    h->test_stall = on;
     return QG_OK;
 }
 

@@ -289,6 +289,29 @@ __global__ void k_mirror_lower(T* __restrict__ A, int ld, int k) {
     }
 }
 
+// Steady-state Gram pencil of [x r p] (column-major, pitch k3 = 3n, lower triangle read
+// by the eigensolvers): the x/p blocks come from the previous iteration's rotation,
+// U = [Bxx | Bxp | Bpp] (n x n each, ld n, before normalisation) scaled by the
+// normalisation factors fx (of x) and fp (of p):
+//   S(x,x) = fx Bxx fx,  S(p,x) = fp Bxp^T fx,  S(p,p) = fp Bpp fp;
+// the r column block was just formed from tall products; its x rows are copied into
+// the (r,x) block of the lower triangle. One block per column j < n.
+__global__ void k_place_blocks(double* __restrict__ S, int k3, int n, const double* __restrict__ U,
+                               const double* __restrict__ fx, const double* __restrict__ fp) {
+    const int j = blockIdx.x;
+    const double* Bxx = U;
+    const double* Bxp = U + (size_t)n * n;
+    const double* Bpp = U + 2 * (size_t)n * n;
+    const double fxj = fx[j], fpj = fp[j];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double xx = fx[i] * Bxx[i + (size_t)j * n] * fxj;
+        S[i + (size_t)j * k3] = xx;
+        S[(2 * n + i) + (size_t)j * k3] = fp[i] * Bxp[j + (size_t)i * n] * fxj;                 // p_i . x_j
+        S[(2 * n + i) + (size_t)(2 * n + j) * k3] = fp[i] * Bpp[i + (size_t)j * n] * fpj;
+        S[(n + i) + (size_t)j * k3] = S[j + (size_t)(n + i) * k3];                               // r_i . x_j
+    }
+}
+
 // T(:, j) = V(:, f + j) / sqrt(s[f + j]) for the kp eigenvectors of B kept.
 template <typename T>
 __global__ void k_scaled_basis(const T* __restrict__ V, int ld, int k, const double* __restrict__ s, int f,
@@ -352,6 +375,9 @@ struct Solver {
     cusolverDnHandle_t sol;
     DevBuf W, AW, T, S, E, small, work, heg;  // heg: batched complex pencils (k-point solve)
     DevBuf gts;                                // partial sums of the tall-skinny Gram kernel
+    DevBuf upd;                                // steady-state Gram reuse: blocks, products, factors
+    double *UA = nullptr, *UB = nullptr, *Tu = nullptr, *fx_d = nullptr, *fp_d = nullptr;
+    bool have_update = false;                  // UA/UB hold the rotated x/p blocks of the last step
     int lwork = 0;
     double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *Sa, *Sb, *Sa2, *Sb2, *M;
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
@@ -366,7 +392,7 @@ struct Solver {
 
     ~Solver() {
         W.release(); AW.release(); T.release(); S.release(); E.release(); small.release();
-        work.release(); heg.release(); gts.release();
+        work.release(); heg.release(); gts.release(); upd.release();
     }
 
     int setup() {
@@ -415,6 +441,55 @@ struct Solver {
         QG_TRY(h->coef.reserve((c == 1 ? qg::coef_scratch_elems(h, n) : qg::coef_scratch_elems_z(h, 1, n)) *
                                sizeof(double)));
         if (mixed) QG_TRY(mg.setup(N, (int)g3, mixed_pieces));
+        if (c == 1) {
+            const size_t nn = (size_t)n * n;
+            QG_TRY(upd.reserve((6 * nn + 2 * k3 * (size_t)n + 2 * (size_t)n) * sizeof(double)));
+            UA = upd.as<double>();
+            UB = UA + 3 * nn;
+            Tu = UB + 3 * nn;
+            fx_d = Tu + 2 * k3 * (size_t)n;
+            fp_d = fx_d + n;
+        }
+        return QG_OK;
+    }
+
+    // Gram pencil of the steady-state step from the previous rotation (the "direct
+    // update" of NextMatrix_d, lobpcg_d_multi_mpi.h:264-460): only the r column block is
+    // a tall product, W^T Ar dV and W^T r dV over W = [x r p] (2 * 2 N 3n n flops against
+    // 2 N (3n)^2 for the full lower triangles); the x/p blocks come from prepare_update.
+    int gram_update(int k3) {
+        QG_TRY(gemm_tn(k3, n, x, Ar, dV, Sa + (size_t)n * k3, k3));
+        QG_TRY(gemm_tn(k3, n, x, r, dV, Sb + (size_t)n * k3, k3));
+        k_place_blocks<<<n, 128, 0, st>>>(Sa, k3, n, UA, fx_d, fp_d);
+        k_place_blocks<<<n, 128, 0, st>>>(Sb, k3, n, UB, fx_d, fp_d);
+        QG_CUDA_TRY(cudaGetLastError());
+        return QG_OK;
+    }
+
+    // After a pencil solve on the k3 x k3 pair (Sa, Sb, lower triangles, pitch k3) with
+    // rotation Z (k3 x n, ld ldz; rows x, r[, p]): the pair of the rotated blocks
+    // x' = [x r p] Z and p' = [r p] Z(n:, :) before normalisation,
+    //   Bxx = Z^T S Z,  Bxp = Z^T S(:, n:) Z(n:, :),  Bpp = Z(n:, :)^T S(n:, n:) Z(n:, :),
+    // for S = Sa (into UA) and S = Sb (into UB).
+    int prepare_update(const double* Z, int ldz, int k3) {
+        const double one = 1.0, zero = 0.0;
+        const int kr = k3 - n;
+        const size_t nn = (size_t)n * n;
+        for (int w = 0; w < 2; ++w) {
+            double* S = w ? Sb : Sa;
+            double* U = w ? UB : UA;
+            k_mirror_lower<double><<<k3, 128, 0, st>>>(S, k3, k3);
+            double* T1 = Tu;
+            double* T2 = Tu + (size_t)k3 * n;
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k3, n, k3, &one, S, k3, Z, ldz, &zero, T1, k3));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, k3, n, kr, &one, S + (size_t)n * k3, k3, Z + n, ldz,
+                                    &zero, T2, k3));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, k3, &one, Z, ldz, T1, k3, &zero, U, n));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, k3, &one, Z, ldz, T2, k3, &zero, U + nn, n));
+            QG_BLAS_TRY(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, kr, &one, Z + n, ldz, T2 + n, k3, &zero,
+                                    U + 2 * nn, n));
+        }
+        QG_CUDA_TRY(cudaGetLastError());
         return QG_OK;
     }
 
@@ -621,6 +696,14 @@ struct Solver {
     }
 };
 
+// Full Gram pencil every this many iterations in steady state (the reference recomputes
+// every S_MAT_REST_LIMIT = 10, lobpcg_d_multi_mpi.h:926, :1040-1043).
+constexpr int kFullGramEvery = 10;
+// Largest |1 - |x'_j|^2 dV| of a rotated Ritz vector before the step is rolled back, and
+// the rollbacks a solve may take before it stops (QG_ERR_CHOLESKY).
+constexpr double kNormDrift = 1.0e-3;
+constexpr int kMaxRollbacks = 20;
+
 int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps, double* ev, double* X_dev,
                double* P_dev, const double* X_host, double* Xout_host, const double* P_host, double* Pout_host,
                qg_lobpcg_report* rep) {
@@ -676,6 +759,20 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     else QG_TRY(s.applyH(s.p, s.Ap));
     s.coldot(s.x, s.Ax, s.dV, s.ev_d);
     s.residual();
+    {
+        // non-finite input states (or P): stop before any pencil is formed from them
+        std::vector<double> r0(n), e0(n);
+        QG_CUDA_TRY(cudaMemcpyAsync(r0.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaMemcpyAsync(e0.data(), s.ev_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int j = 0; j < n; ++j)
+            if (!std::isfinite(r0[j]) || !std::isfinite(e0[j])) {
+                cudaEventDestroy(t0);
+                cudaEventDestroy(t1);
+                qg_set_last_error("run_lobpcg", "non-finite value in the initial states", __FILE__, __LINE__);
+                return QG_ERR_NONFINITE;
+            }
+    }
     qg::KineticPrecond* pc = nullptr;
     const bool learned = opt->precond == 2;
     // w = T r (precond 1), w = T r + NN(r) (precond 2: the learned correction, learned.cu)
@@ -706,18 +803,26 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     bool converged = false;
     double maxres = 0.0;
     int status = QG_OK;
-    int restarts = 0;
+    int restarts = 0, rollbacks = 0;
     const int c = comps;
     const int nconv = (opt->n_converge > 0 && opt->n_converge < n) ? opt->n_converge : n;
     double best_res = 1e300;
     int best_it = 0, mixed_iters = s.mixed ? opt->max_iter : 0;
+    bool restart_2n = false;  // after a norm-drift rollback: the next step uses the [x r] pencil
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
         tm.mark(1, st);
-        const bool two = first && it == 0;
+        const bool two = (first && it == 0) || restart_2n;
+        restart_2n = false;
         const int k3 = (two ? 2 : 3) * n;
-        QG_TRY(s.gram(c * k3));
+        // steady state: the x/p blocks of the pencil come from the last rotation and only
+        // the r blocks are tall products; a full Gram every kFullGramEvery iterations, after
+        // a 2n step, a rank-revealing solve or a rollback, and in the reduced-precision phase
+        const bool use_update = s.have_update && !two && !s.mixed && (it % kFullGramEvery) != 0;
+        if (use_update) QG_TRY(s.gram_update(k3));
+        else QG_TRY(s.gram(c * k3));
+        s.have_update = false;
         tm.mark(2, st);
         // Jacobi-equilibrated pencil (keeps the tiny residual columns of the reference
         // iteration from ruining the Cholesky factor of B), cuSOLVER sygvd / hegvd on it;
@@ -747,14 +852,47 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         // and the A-side blocks are re-applied, Ax = H x_new, Ap = H p_new, instead of
         // rotated: two memory-bound H applications cost less than the two tall DGEMMs
         // and keep Ax consistent with x for the residual.
+        const bool next_update = h->gram_reuse && c == 1 && !s.mixed && !restarted && 3 * n > qg::kGramTsUpTo;
+        if (next_update) QG_TRY(s.prepare_update(Z, ldz, k3));
         QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp, 0.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_TRY(s.gemm_nn(c * n, c * n, s.x, Z, ldz, s.Tx, 1.0));
+        // norm drift of the rotated x (B-normalised Ritz vectors have |x'|^2 dV = 1): beyond
+        // 1e-3 the step is rolled back -- x and p stay, and the next step solves the [x r]
+        // pencil with a full Gram (the rollback of Eigen_d_multi_mpi, lobpcg_d_multi_mpi.h:1305-1346,
+        // which keeps X and stops; here the iteration goes on from the kept X)
+        s.coldot(s.Tx, s.Tx, 1.0, s.nr_d);
+        QG_CUDA_TRY(cudaMemcpyAsync(nr_h.data(), s.nr_d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QG_CUDA_TRY(cudaStreamSynchronize(st));
+        double drift = 0.0;
+        for (int j = 0; j < n; ++j) drift = std::max(drift, std::fabs(1.0 - nr_h[j] * s.dV));
+        if (!(drift <= kNormDrift) && !two) {
+            ++restarts;
+            ++rollbacks;
+            restart_2n = true;
+            s.have_update = false;
+            if (opt->verbose) printf("lobpcg iter %d: |x|^2 drift %.3e, rolled back\n", it + 1, drift);
+            tm.mark(-1, st);
+            QG_CUDA_TRY(cudaStreamSynchronize(st));
+            tm.flush();
+            if (rollbacks > kMaxRollbacks) {
+                status = QG_ERR_CHOLESKY;
+                ++it;
+                break;
+            }
+            continue;
+        }
         QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         tm.mark(4, st);
-        s.normalize(s.x, nullptr);
+        k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, s.dV, n, s.f_d);  // norms of x' taken above
+        s.scale_cols(s.x, nullptr);
+        if (next_update) QG_CUDA_TRY(cudaMemcpyAsync(s.fx_d, s.f_d, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         s.normalize(s.p, nullptr);
+        if (next_update) {
+            QG_CUDA_TRY(cudaMemcpyAsync(s.fp_d, s.f_d, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            s.have_update = true;
+        }
         tm.mark(0, st);
         QG_TRY(s.applyH(s.x, s.Ax));
         QG_TRY(s.applyH(s.p, s.Ap));
@@ -1198,6 +1336,12 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
 }  // namespace
 
 extern "C" {
+
+int qg_hamiltonian_set_gram_reuse(qg_hamiltonian h, int on) {
+    if (!h || (on != 0 && on != 1)) return QG_ERR_INVALID;
+    h->gram_reuse = on;
+    return QG_OK;
+}
 
 int qg_lobpcg_d(qg_hamiltonian h, const qg_lobpcg_options* opt, int ns, double* ev, double* X, double* P,
                 qg_lobpcg_report* rep) {

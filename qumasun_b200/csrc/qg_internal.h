@@ -129,6 +129,8 @@ struct qg_hamiltonian_s {
     int proj_sb = 0;     // states per projection block (0: chosen per launch)
     int proj_parts = 0;  // blocks (one cluster) per atom in the projection (0: from the cell)
     int scatter_sg = 0;  // states per scatter group (0: 8)
+    int test_stall = 0;  // test hook: ring-stencil producers issue nothing (bounded waits run out)
+    int gram_reuse = 1;  // LOBPCG: steady-state Gram pencil from the last rotation (0: full Gram every step)
     qg::KineticPrecond* precond = nullptr;  // LOBPCG preconditioner, built on first use
     qg_learned learned = nullptr;           // network of precond = 2 (qg_hamiltonian_set_learned)
     double learned_vscale = 1.0;

@@ -25,6 +25,8 @@ struct HamArgs {
     long long ldc;   // coefficient row length (states, padded to 16)
     const T* coef;   // [na * nch][ldc]
     int* err;        // device status word: nonzero after a bounded wait gave up
+    int stall;       // test hook: the ring kernels' producer issues nothing, so the
+                     // consumers' bounded waits run out (QG_ERR_TIMEOUT)
     // complex (k-point) states: the imaginary part of a state starts xim (hxim)
     // elements after its real part; dx/dy/dz are the 8th-order first-derivative
     // coefficients 2*coef*g/(840h)*(672, -168, 32, -3) per axis (zero for an

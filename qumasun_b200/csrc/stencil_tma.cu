@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
 
     if (t < 32) {
         // ---------------- producer warp: lane 0 streams planes ----------------
-        if (t == 0) {
+        if (t == 0 && !a.stall) {
             int pos = 0;
             for (int item = blockIdx.x; item < wg.items && !ctl[0]; item += gridDim.x) {
                 const int slab = item % wg.nslab;

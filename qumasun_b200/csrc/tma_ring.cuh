@@ -79,17 +79,20 @@ struct WorkGrid {
 // same copy, split where the tile wraps periodically in y), into ring stage
 // pos % nst, pos counting planes over all items. A stage is refilled only after
 // every consumer warp has arrived on its "empty" barrier. NC = 2 copies the real and
-// the imaginary part of each plane into one stage. On a wait that gives up, sets
-// ctl[0] and the device status word and stops; ctl[1] = last position issued.
-template <typename T, int R, int NC>
+// the imaginary part of each plane into one stage. WITHV: each stage also carries, after
+// the state rows, the ty rows of the local potential of that plane (the tile's own rows,
+// one contiguous copy). On a wait that gives up, sets ctl[0] and the device status word
+// and stops; ctl[1] = last position issued.
+template <typename T, int R, int NC, bool WITHV = false>
 __device__ void produce_planes(const HamArgs<T>& a, const WorkGrid& wg, int nst, int nx, T* ringp,
                                uint64_t* full, uint64_t* empty, volatile int* ctl) {
     const int ny = a.ny, nz = a.nz, ty = a.ty;
     const int rows = ty + 2 * R;
     const int comp_elems = rows * nx;
-    const int stage_elems = NC * comp_elems;
+    const int stage_elems = NC * comp_elems + (WITHV ? ty * nx : 0);
     const uint32_t stage_bytes = (uint32_t)stage_elems * sizeof(T);
     const long long plane = (long long)nx * ny;
+    if (a.stall) return;
     int pos = 0;
     for (int item = blockIdx.x; item < wg.items && !ctl[0]; item += gridDim.x) {
         const int slab = item % wg.nslab;
@@ -123,6 +126,9 @@ __device__ void produce_planes(const HamArgs<T>& a, const WorkGrid& wg, int nst,
                     r += cnt;
                 }
             }
+            if constexpr (WITHV)
+                bulk_g2s(dst + (size_t)NC * comp_elems, a.V + zoff + (long long)y0 * nx, (uint32_t)(ty * nx * sizeof(T)),
+                         &full[j]);
             ctl[1] = pos;
         }
     }
@@ -130,8 +136,8 @@ __device__ void produce_planes(const HamArgs<T>& a, const WorkGrid& wg, int nst,
 
 // Ring stages of `stage_bytes` that fit the shared-memory budget (at least
 // max(2R, R + extra) stages), or -1.
-inline int ring_stages(int R, size_t stage_bytes, int extra = 2) {
-    const size_t budget = 200 * 1024 - kBarBytes;
+inline int ring_stages(int R, size_t stage_bytes, int extra = 2, size_t budget_kb = 200) {
+    const size_t budget = budget_kb * 1024 - kBarBytes;
     int nst = (int)((budget / stage_bytes) < (size_t)kMaxStages ? budget / stage_bytes : kMaxStages);
     const int need = 2 * R > R + extra ? 2 * R : R + extra;
     return nst >= need ? nst : -1;

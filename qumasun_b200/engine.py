@@ -119,6 +119,8 @@ def lib():
         L.qg_hamiltonian_launches_per_apply.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_set_stencil_kernel.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_set_nonlocal_blocking.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.qg_hamiltonian_set_gram_reuse.argtypes = [vp, C.c_int]
+        L.qg_hamiltonian_test_stall.argtypes = [vp, C.c_int]
         L.qg_context_take_device_status.argtypes = [vp]
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
@@ -697,6 +699,10 @@ class Hamiltonian:
         atom in the projection (1-8); 0 = engine's choice."""
         check(lib().qg_hamiltonian_set_nonlocal_blocking(self.h, project_states, scatter_states, project_parts),
               "qg_hamiltonian_set_nonlocal_blocking")
+
+    def set_gram_reuse(self, on: bool):
+        """Steady-state Gram pencil from the previous rotation (True, default) or a full Gram every step."""
+        check(lib().qg_hamiltonian_set_gram_reuse(self.h, 1 if on else 0), "qg_hamiltonian_set_gram_reuse")
 
     def launches_per_apply(self, ns):
         return lib().qg_hamiltonian_launches_per_apply(self.h, ns)

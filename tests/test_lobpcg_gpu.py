@@ -125,3 +125,77 @@ def test_cells_solved_together_match_one_by_one(cuda_ctx):
         h.close()
     for c in ctxs:
         c.close()
+
+
+def test_gram_reuse_reaches_the_full_gram_eigenpairs(cuda_ctx):
+    """More than 128 Gram columns (64-atom 80^3 cell, 60 states, 48 judged): the steady-state
+    pencil from the last rotation (direct update, full Gram every 10 iterations) reaches
+    the eigenvalues of the full-Gram iteration to 1e-9 Ha, both converged."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(reps=(2, 2, 2), displacement=0.05, seed=11)
+    X0 = initial_states(60, cell.N, seed=12)
+    H = Hamiltonian(cuda_ctx, cell)
+    out = {}
+    for reuse in (True, False):
+        H.set_gram_reuse(reuse)
+        X = torch.from_numpy(X0).cuda()
+        r = H.lobpcg_device(X, None, max_iter=400, precond=1, n_converge=48)
+        assert r["status"] == 0 and r["report"]["converged"] == 1, (reuse, r["report"])
+        out[reuse] = r
+    d = np.abs(out[True]["ev"][:48] - out[False]["ev"][:48]).max()
+    assert d < 1e-9, d
+    it_r, it_f = out[True]["report"]["iterations"], out[False]["report"]["iterations"]
+    assert it_r <= it_f + 10, (it_r, it_f)
+    H.set_gram_reuse(True)
+    H.close()
+
+
+def test_nonfinite_start_reports_nonfinite(cuda_ctx):
+    from qumasun_b200 import Hamiltonian, QGError
+    cell = build_cell(grid=(16, 16, 16))
+    X0 = initial_states(4, cell.N, seed=3)
+    X0[2, 100] = np.nan
+    H = Hamiltonian(cuda_ctx, cell)
+    with pytest.raises(QGError) as e:
+        H.lobpcg(X0, max_iter=50)
+    assert e.value.status == -6  # QG_ERR_NONFINITE
+    # the operator and context stay usable
+    r = H.lobpcg(initial_states(4, cell.N, seed=3), max_iter=500)
+    assert r["status"] == 0
+    H.close()
+
+
+def test_rank_deficient_start_reports_cholesky(cuda_ctx):
+    """Every starting state the same vector: [x r p] spans one direction per block, fewer
+    than ns independent directions remain in the pencil."""
+    from qumasun_b200 import Hamiltonian, QGError
+    cell = build_cell(grid=(16, 16, 16))
+    X0 = np.repeat(initial_states(1, cell.N, seed=5), 4, axis=0)
+    H = Hamiltonian(cuda_ctx, cell)
+    with pytest.raises(QGError) as e:
+        H.lobpcg(X0, max_iter=50)
+    assert e.value.status == -4  # QG_ERR_CHOLESKY
+    H.close()
+
+
+def test_bounded_stencil_wait_reports_timeout_and_context_survives(cuda_ctx):
+    """The test hook keeps the ring stencil's producer from issuing any copy: every consumer
+    wait runs out (about 2^31 SM clocks), the kernel winds down and records
+    QG_ERR_TIMEOUT; after the hook is cleared the same operator gives the oracle's H|psi>."""
+    import torch
+    from qumasun_b200 import Hamiltonian, lib
+    cell = build_cell(grid=(24, 24, 24))
+    X = initial_states(3, cell.N, seed=4)
+    H = Hamiltonian(cuda_ctx, cell)
+    Xd = torch.from_numpy(X).cuda()
+    assert lib().qg_hamiltonian_test_stall(H.h, 1) == 0
+    H.apply(Xd)
+    torch.cuda.synchronize()
+    assert cuda_ctx.take_device_status() == -5  # QG_ERR_TIMEOUT
+    assert lib().qg_hamiltonian_test_stall(H.h, 0) == 0
+    out = H.apply(Xd).cpu().numpy()
+    ref = O.hamiltonian_apply(cell, X)
+    assert (np.linalg.norm(out - ref, axis=1) / np.linalg.norm(ref, axis=1)).max() < 1e-12
+    assert cuda_ctx.take_device_status() == 0
+    H.close()
