@@ -32,10 +32,11 @@ sys.path.insert(0, ROOT)
 
 NS = 256
 REPS = (2, 2, 2)
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_stencil_tma launch per
-# state of this workload, from an ncu --set full capture of the same bench at 32 states
-# (229.9 MB / 32); traffic grows in proportion to the states, so a full launch is scaled.
-STENCIL_DRAM_BYTES_PER_STATE = 229949440 / 32
+# The dominant kernel of the apply and its DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) per state of this workload, from an ncu capture of the same bench
+# at 32 states; traffic grows in proportion to the states, so a full launch is scaled.
+STENCIL_KERNEL = "k_stencil_rows<double, 8, 80> (FD stencil + V, two rows per thread, V in the ring)"
+STENCIL_DRAM_BYTES_PER_STATE = None
 FD_ORDER = 8
 WORKLOAD = "diamond64_80cube_Hpsi"
 
@@ -56,6 +57,10 @@ def parse():
     p.add_argument("--no-kpoint", action="store_true", help="skip the k-point leg (64 Monkhorst-Pack points)")
     p.add_argument("--no-cells", action="store_true",
                    help="skip the 16-cell leg (8- to 64-atom cells solved one by one and together)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the engine's default launch shapes (profiling captures)")
+    p.add_argument("--no-scf", action="store_true",
+                   help="skip the SCF-step leg (density, potential, Taylor-4 step, nonlocal forces)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-preconditioner leg (GPU training and an unseen-cell comparison)")
     p.add_argument("--only", choices=["kpoint", "gram", "cells"], default=None,
@@ -555,6 +560,79 @@ def lobpcg_diamond216(ctx):
             "speedup_fp32_gram_vs_fp64": round(runs["fp64"]["seconds"] / runs["fp32_gram"]["seconds"], 3)}
 
 
+def scf_leg(ctx, X, cell, steps=10, cpu=True):
+    """The SCF-step neighbours of the eigensolver on the 64-atom 80^3 cell: density of the
+    256 states (qg_density_d), the Poisson + LDA potential (qg_potential_lda_d) at 80^3 and
+    120^3, one Taylor-4 step of 64 complex states (qg_td_taylor4_z: four H applications
+    and the updates) and the nonlocal energies and forces of the 256 states
+    (qg_nonlocal_force_d); device times by CUDA events. With cpu=True the reference's
+    TimeEvoH4 and ForceNonlocal (oracle/_ref) are timed on one state each, single-thread."""
+    import numpy as np
+    import torch
+    from qumasun_b200 import Hamiltonian, Poisson, density
+    from qumasun_b200.cell import build_cell, initial_states
+    ns, N = X.shape
+    occ = np.where(np.arange(ns) < 128, 2.0, 0.0)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": "diamond64_80cube_scf_step_neighbours"}
+    rho = torch.zeros(N, dtype=torch.float64, device="cuda")
+    ms = timed(lambda: density(ctx, X, occ, rho=rho), steps)
+    nocc = int((occ > 0).sum())
+    out["density"] = {"states": ns, "occupied": nocc, "ms": round(ms, 4),
+                      "GBs": round((nocc * N * 8 + N * 8) / (ms * 1e-3) / 1e9, 1)}
+    pot = {}
+    for reps_ in ((2, 2, 2), (3, 3, 3)):
+        c = build_cell(reps=reps_)
+        P = Poisson(ctx, (c.nx, c.ny, c.nz), (c.hx, c.hy, c.hz))
+        r = torch.from_numpy(0.02 + 0.3 * np.exp(c.V / 4.0)).cuda()
+        v = torch.from_numpy(c.V).cuda()
+        pot[f"{c.nx}cube"] = {"ms": round(timed(lambda: P.potential(r, v), steps), 4)}
+        P.close()
+    out["potential_lda"] = pot
+    Hk = Hamiltonian(ctx, cell, kvec=(0.0582, 0.0582, 0.0582))
+    Z = (torch.rand(64, 2 * N, dtype=torch.float64, device="cuda") - 0.5) * 1e-2
+    ms = timed(lambda: Hk.td_taylor4(Z, 0.002), 3)
+    out["taylor4"] = {"states": 64, "ms_per_step": round(ms, 3), "state_steps_per_s": round(64 / (ms * 1e-3), 1)}
+    Hk.close()
+    H = Hamiltonian(ctx, cell)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f, e, ev = H.nonlocal_force(X, occ)
+    out["nonlocal_force"] = {"states": ns, "occupied": nocc, "seconds": round(time.perf_counter() - t0, 4),
+                             "ev_sum_Ha": ev}
+    H.close()
+    if cpu:
+        try:
+            import oracle as O
+            Z1 = initial_states(1, 2 * N, seed=5) * 1e-2
+            t1 = time.perf_counter()
+            O.td_taylor4(cell, (0.0582, 0.0582, 0.0582), 0.002, Z1, impl="ref")
+            tt = time.perf_counter() - t1
+            X1 = X[:1].cpu().numpy()
+            t1 = time.perf_counter()
+            O.nonlocal_force(cell, X1, np.array([2.0]), impl="ref")
+            tf = time.perf_counter() - t1
+            out["reference_cpu"] = {"taylor4_s_per_state": round(tt, 3), "force_s_per_state": round(tf, 3),
+                                    "cores": 1, "kind": "reference",
+                                    "sample": "QUMASUN::TimeEvoH4 and ForceNonlocal (with Gradient8th) on one "
+                                              "state of the 80^3 64-atom cell, single thread"}
+            out["speedup_taylor4_vs_reference_cpu_per_state"] = round(tt / (ms * 1e-3 / 64), 1)
+        except Exception as ex:
+            out["reference_cpu"] = {"failed": str(ex)}
+    return out
+
+
 # --------------------------------------------------------------- GPU arm
 def run_gpu_arm(a):
     import numpy as np
@@ -599,6 +677,13 @@ def run_gpu_arm(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # the engine's autotuner picks the bit-identical launch shapes on these states
+    tuned = None
+    if not a.no_autotune:
+        with torch.cuda.stream(stream):
+            tuned = H.autotune(X, HX)
+    stream.synchronize()
+    ctx.set_stream(stream.cuda_stream)
     # warm-up
     for _ in range(max(3, a.warmup)):
         H.apply_device(NS, X.data_ptr(), HX.data_ptr())
@@ -624,7 +709,7 @@ def run_gpu_arm(a):
     # dominant-kernel roofline: per-phase device times of one apply
     phases = sorted((H.apply_timed(NS, X.data_ptr(), HX.data_ptr()) for _ in range(5)), key=lambda p: p[1])
     ms_proj, ms_sten, ms_scat = phases[2]
-    # k_stencil_tma: psi in, H psi out, V, and the scatter-side projector entries once
+    # the stencil kernel: psi in, H psi out, V once
     sten_bytes = N * NS * 2 * 8 + N * 8
     peak, peak_kind = measured_peak_hbm()
     sten_gbs = sten_bytes / (ms_sten * 1e-3) / 1e9
@@ -688,6 +773,9 @@ def run_gpu_arm(a):
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
+    scf = None
+    if solo and not a.no_scf:
+        scf = scf_leg(ctx, X, cell, cpu=not a.no_cpu_baseline)
     kp = None
     if not a.no_kpoint:
         kp = kpoint_leg(ctx, n_k=a.kpoints, rank=rank, ws=ws)
@@ -714,12 +802,14 @@ def run_gpu_arm(a):
             "data": "synthetic",
             "config": bench_config(cell, ws),
             "state_applications_per_s": round(NS * ws / (ms_max * 1e-3), 1),
-            "roofline": {"bound": "hbm", "kernel": "k_stencil_tma (FD stencil + V)",
+            "autotuned": tuned,
+            "roofline": {"bound": "hbm", "kernel": STENCIL_KERNEL,
                          "achieved": round(sten_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(sten_gbs / peak, 4), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": sten_bytes, "launches": 1,
                          "ms_per_launch": round(ms_sten, 5),
-                         "traffic": int(STENCIL_DRAM_BYTES_PER_STATE * NS),
+                         "traffic": (int(STENCIL_DRAM_BYTES_PER_STATE * NS) if STENCIL_DRAM_BYTES_PER_STATE
+                                     else None),
                          "traffic_note": "ncu capture at 32 states scaled by states",
                          "phase_ms_per_apply": phase_ms,
                          "whole_apply_frac": round(gbs / peak, 4)},
@@ -736,6 +826,8 @@ def run_gpu_arm(a):
             line["lobpcg_216"] = lob216
         if kp:
             line["kpoint"] = kp
+        if scf:
+            line["scf"] = scf
         if lrn:
             line["learned_preconditioner"] = lrn
         if cells_res:

@@ -365,12 +365,14 @@ int qg_hegv_small_batched_z(qg_context ctx, int batch, int k, const double* A, c
                             long long stride, double* w, double* Z, int* info);
 
 /* Selects the stencil kernel of an operator's real-state apply: 0 = the engine's
- * choice (default: the one-plane TMA ring kernel where the shape and alignment
- * allow, else the two-plane ring kernel, else the register-window kernel),
+ * choice (default: the TMA ring kernel with two grid rows per thread where the shape
+ * and alignment allow -- the one-plane ring kernel for FP32 order 2 -- else the other
+ * ring kernels, else the register-window kernel),
  * 1 = always the register-window kernel (any shape), 2 = the one-plane ring
- * kernel, 3 = the two-plane ring kernel (2 and 3 fall back as 0 does where the
- * shape does not fit). All compute the same operator. Complex states use the
- * one-plane ring kernel unless 1 is set. */
+ * kernel, 3 = the two-plane ring kernel, 4 = the ring kernel with two grid rows per
+ * thread and V streamed through the ring (2-4 fall back as 0 does where the shape
+ * does not fit). All give the same bits. Complex states use the one-plane ring kernel
+ * unless 1 is set. */
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int variant);
 /* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
  * complex states use at most 4), states per scatter group of the real apply (4 or
@@ -396,6 +398,20 @@ int qg_hamiltonian_set_gram_reuse(qg_hamiltonian ham, int on);
  * qg_context_take_device_status) and the context stays usable. 0 restores normal
  * operation. Nothing in the library sets it. */
 int qg_hamiltonian_test_stall(qg_hamiltonian ham, int on);
+/* Autotuner of the real-state apply (no counterpart in the reference): times, on the
+ * caller's DEVICE block of ns states (X in, HX overwritten), the launch shapes that leave
+ * every bit of H|psi> unchanged -- stencil kernel (variants 2, 3, 4 of
+ * qg_hamiltonian_set_stencil_kernel), states per projection block (2, 4, 8, 16) and per
+ * scatter group (4, 8) -- one dimension at a time (the phases are independent), best of
+ * three CUDA-event timed applies each, and keeps the fastest in the operator.
+ * choice (3 ints, may be NULL) receives {stencil variant, projection states, scatter
+ * states}; ms_phases (3 floats, may be NULL) the chosen configuration's projection,
+ * stencil + V and scatter times. The projector split over blocks is left to the cell
+ * rule: it changes the summation order. About 40 applies. */
+int qg_hamiltonian_autotune_d(qg_hamiltonian ham, int ns, const double* X, long long ldx, double* HX,
+                              long long ldhx, int* choice, float* ms_phases);
+int qg_hamiltonian_autotune_f(qg_hamiltonian ham, int ns, const float* X, long long ldx, float* HX,
+                              long long ldhx, int* choice, float* ms_phases);
 /* Number of kernel launches one apply of `ns` states issues (for launch accounting). */
 int qg_hamiltonian_launches_per_apply(qg_hamiltonian ham, int ns);
 

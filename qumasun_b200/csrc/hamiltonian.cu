@@ -238,10 +238,10 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const T* __restrict__ 
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int atom = blockIdx.x / chunks;
-    const int s0 = blockIdx.y * SB;
     const int a0 = atom_off[atom], a1 = atom_off[atom + 1];
     const int len = (a1 - a0 + chunks - 1) / chunks;
     const int p0 = min(a1, a0 + rank * len), p1 = min(a1, p0 + len);
+    const int s0 = blockIdx.y * SB;
     T acc[SB][NCH];
 #pragma unroll
     for (int s = 0; s < SB; ++s)
@@ -603,19 +603,27 @@ size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk) {
 }
 
 // Stencil kernel for a real-state apply: the forced variant when it accepts the shape,
-// else the one-plane ring kernel (measured faster than the two-plane one on the 80^3
-// cell at every order: 0.76 against 0.90 ms at order 8), else the two-plane ring
-// kernel, else (1) the register-window kernel, which takes any shape.
+// else the two-row ring kernel (4; measured on the 80^3 cell, 256 states: FP64 order 8
+// 0.553 ms against 0.764 for the one-plane kernel and 0.896 for the two-plane one, and
+// faster at every FP64 order and at FP32 orders 4-8), except FP32 order 2, where the
+// one-plane kernel (2) is faster (0.91 against 1.00 ms for the whole apply); then the
+// one-plane, then the two-plane ring kernel, else (1) the register-window kernel, which
+// takes any shape. All ring kernels give the same bits.
 template <typename T>
 static int ring_stencil_variant(qg_hamiltonian h, const HamArgs<T>& a) {
     const int v = h->stencil_variant;
     if (v == 1) return 1;
     const bool pair_ok = stencil_pair_ok<T>(a, h->order);
     const bool tma_ok = stencil_tma_ok<T>(a, h->order);
+    const bool rows_ok = stencil_rows_ok<T>(a, h->order);
     if (v == 3 && pair_ok) return 3;
     if (v == 2 && tma_ok) return 2;
+    if (v == 4 && rows_ok) return 4;
+    const bool one_plane_first = sizeof(T) == 4 && h->order == 2;
+    if (rows_ok && !(one_plane_first && tma_ok)) return 4;
     if (tma_ok) return 2;
     if (pair_ok) return 3;
+    if (rows_ok) return 4;
     return 1;
 }
 
@@ -673,7 +681,9 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
     const int variant = ring_stencil_variant<T>(h, a);
     if (variant != 1) {
         auto stencil = [&]() {
-            return variant == 3 ? launch_stencil_pair<T>(a, h->order, st) : launch_stencil_tma<T>(a, h->order, st);
+            if (variant == 3) return launch_stencil_pair<T>(a, h->order, st);
+            if (variant == 4) return launch_stencil_rows<T>(a, h->order, st);
+            return launch_stencil_tma<T>(a, h->order, st);
         };
         if (!nonlocal) {
             if (pt) pt->mark(1, st);
@@ -1055,7 +1065,7 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long
 }
 
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int variant) {
-    if (!h || variant < 0 || variant > 3) return QG_ERR_INVALID;
+    if (!h || variant < 0 || variant > 4) return QG_ERR_INVALID;
     h->stencil_variant = variant;
     return QG_OK;
 }

@@ -124,7 +124,8 @@ struct qg_hamiltonian_s {
     cudaStream_t io_in = nullptr, io_out = nullptr;  // copy streams of the host-buffer entry points
     int ty = 1;       // grid rows per stencil tile
     // stencil kernel of the real-state apply: 0 = engine's choice, 1 = register-window
-    // kernel (any shape), 2 = one-plane TMA ring, 3 = two-plane TMA ring
+    // kernel (any shape), 2 = one-plane TMA ring, 3 = two-plane TMA ring, 4 = two rows per
+    // thread with V in the ring
     int stencil_variant = 0;
     int proj_sb = 0;     // states per projection block (0: chosen per launch)
     int proj_parts = 0;  // blocks (one cluster) per atom in the projection (0: from the cell)
@@ -202,8 +203,10 @@ inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 bloc
 // each block's serial walk over its points sets the time) one per kProjPartPoints
 // sphere points of the largest atom, at most 8 (the portable cluster size). Measured on
 // 8-, 64- and 216-atom diamond cells at 16-256 real and 16-128 complex states; on the
-// large cells 2 parts were within 2 % of 1 and changed the last bits of H enough to
-// take the 216-atom LOBPCG (480 of 528 states) from 40 to 102 iterations.
+// large cells 2 parts were within 2 % of 1. Two parts per atom with every block walking
+// all state groups in turn (so that all atoms sweep the groups together and the sphere
+// overlaps hit L2) measured slower on the 64-atom cell, 0.69 against 0.49 ms at 256
+// states: 128 blocks hide less gather latency than 2048 (atom, group) blocks.
 constexpr int kProjPartPoints = 4096;
 inline int project_parts(const DevProjectors& pj, int forced) {
     if (forced > 0) return forced;

@@ -66,5 +66,10 @@ template <typename T>
 int launch_stencil_pair(const HamArgs<T>& a, int order, cudaStream_t st);
 template <typename T>
 bool stencil_pair_ok(const HamArgs<T>& a, int order);
+// Real states, two grid rows per consumer thread, V streamed through the ring (stencil_rows.cu).
+template <typename T>
+int launch_stencil_rows(const HamArgs<T>& a, int order, cudaStream_t st);
+template <typename T>
+bool stencil_rows_ok(const HamArgs<T>& a, int order);
 
 }  // namespace qg

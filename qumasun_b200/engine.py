@@ -121,6 +121,10 @@ def lib():
         L.qg_hamiltonian_set_nonlocal_blocking.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.qg_hamiltonian_set_gram_reuse.argtypes = [vp, C.c_int]
         L.qg_hamiltonian_test_stall.argtypes = [vp, C.c_int]
+        L.qg_hamiltonian_autotune_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong, _ip,
+                                                C.POINTER(C.c_float)]
+        L.qg_hamiltonian_autotune_f.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong, _ip,
+                                                C.POINTER(C.c_float)]
         L.qg_context_take_device_status.argtypes = [vp]
         L.qg_hamiltonian_apply_noalloc_d.argtypes = [vp, C.c_int, vp, C.c_longlong, vp, C.c_longlong]
         L.qg_noalloc_scratch_capacity.restype = C.c_size_t
@@ -690,7 +694,8 @@ class Hamiltonian:
 
     def set_stencil_kernel(self, variant):
         """Stencil kernel of the real-state apply: 0 (or False) = engine's choice, 1 (or
-        True) = register-window kernel, 2 = one-plane TMA ring, 3 = two-plane TMA ring."""
+        True) = register-window kernel, 2 = one-plane TMA ring, 3 = two-plane TMA ring,
+        4 = two rows per thread with V in the ring."""
         v = int(variant)
         check(lib().qg_hamiltonian_set_stencil_kernel(self.h, v), "qg_hamiltonian_set_stencil_kernel")
 
@@ -699,6 +704,23 @@ class Hamiltonian:
         atom in the projection (1-8); 0 = engine's choice."""
         check(lib().qg_hamiltonian_set_nonlocal_blocking(self.h, project_states, scatter_states, project_parts),
               "qg_hamiltonian_set_nonlocal_blocking")
+
+    def autotune(self, X, out=None):
+        """Times the bit-identical launch shapes on the CUDA block X (float64 or float32,
+        (ns, N)) and keeps the fastest; returns dict(stencil, project_states,
+        scatter_states, ms_phases)."""
+        import torch
+        self._check_block(X, "X", (torch.float64, torch.float32))
+        out = torch.empty_like(X) if out is None else out
+        self._check_block(out, "out", (X.dtype,))
+        choice = (C.c_int * 3)()
+        ms = (C.c_float * 3)()
+        fn = lib().qg_hamiltonian_autotune_d if X.dtype == torch.float64 else lib().qg_hamiltonian_autotune_f
+        self.ctx.use_torch_stream()
+        check(fn(self.h, X.shape[0], _dev(X), X.shape[1], _dev(out), out.shape[1], choice, ms),
+              "qg_hamiltonian_autotune")
+        return dict(stencil=choice[0], project_states=choice[1], scatter_states=choice[2],
+                    ms_phases=[round(float(v), 4) for v in ms])
 
     def set_gram_reuse(self, on: bool):
         """Steady-state Gram pencil from the previous rotation (True, default) or a full Gram every step."""

@@ -199,3 +199,28 @@ def test_bounded_stencil_wait_reports_timeout_and_context_survives(cuda_ctx):
     assert (np.linalg.norm(out - ref, axis=1) / np.linalg.norm(ref, axis=1)).max() < 1e-12
     assert cuda_ctx.take_device_status() == 0
     H.close()
+
+
+def test_config2_cell_mixed_precision_matches_fp64(cuda_ctx):
+    """The mixed-precision configuration's cell (216 atoms, 120^3, sigma 0.05 bohr): 64
+    states (the lowest 48 judged, a 16-state guard band), kinetic preconditioner, FP64
+    against split-BF16x3 and FP32 Gram products -- the same 48 eigenvalues to 1e-8 Ha,
+    all converged, the reduced precisions having run some iterations."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(reps=(3, 3, 3), displacement=0.05, seed=2024)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    X0 = torch.rand(64, cell.N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    H = Hamiltonian(cuda_ctx, cell)
+    ev = {}
+    for prec in (0, 2, 1):
+        X = X0.clone()
+        r = H.lobpcg_device(X, None, max_iter=300, precond=1, n_converge=48, precision=prec)
+        assert r["status"] == 0 and r["report"]["converged"] == 1, (prec, r["report"])
+        if prec:
+            assert r["report"]["mixed_iterations"] > 0
+        ev[prec] = r["ev"][:48]
+        del X
+    H.close()
+    for prec in (2, 1):
+        assert np.abs(ev[prec] - ev[0]).max() < 1e-8, (prec, np.abs(ev[prec] - ev[0]).max())
