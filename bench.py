@@ -36,7 +36,7 @@ REPS = (2, 2, 2)
 # dram__bytes_write.sum) per state of this workload, from an ncu capture of the same bench
 # at 32 states; traffic grows in proportion to the states, so a full launch is scaled.
 STENCIL_KERNEL = "k_stencil_rows<double, 8, 80> (FD stencil + V, two rows per thread, V in the ring)"
-STENCIL_DRAM_BYTES_PER_STATE = None
+STENCIL_DRAM_BYTES_PER_STATE = (138647296 + 92578048) / 32
 FD_ORDER = 8
 WORKLOAD = "diamond64_80cube_Hpsi"
 

@@ -366,12 +366,12 @@ int qg_hegv_small_batched_z(qg_context ctx, int batch, int k, const double* A, c
 
 /* Selects the stencil kernel of an operator's real-state apply: 0 = the engine's
  * choice (default: the TMA ring kernel with two grid rows per thread where the shape
- * and alignment allow -- the one-plane ring kernel for FP32 order 2 -- else the other
- * ring kernels, else the register-window kernel),
+ * and alignment allow -- V through the ring in FP64, from global memory in FP32 -- else
+ * the other ring kernels, else the register-window kernel),
  * 1 = always the register-window kernel (any shape), 2 = the one-plane ring
  * kernel, 3 = the two-plane ring kernel, 4 = the ring kernel with two grid rows per
- * thread and V streamed through the ring (2-4 fall back as 0 does where the shape
- * does not fit). All give the same bits. Complex states use the one-plane ring kernel
+ * thread and V streamed through the ring, 5 = the same with V read one plane ahead from
+ * global memory (2-5 fall back as 0 does where the shape does not fit). All give the same bits. Complex states use the one-plane ring kernel
  * unless 1 is set. */
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian ham, int variant);
 /* Tuning of the nonlocal passes: states per projection block (1, 2, 4, 8 or 16;
@@ -400,7 +400,7 @@ int qg_hamiltonian_set_gram_reuse(qg_hamiltonian ham, int on);
 int qg_hamiltonian_test_stall(qg_hamiltonian ham, int on);
 /* Autotuner of the real-state apply (no counterpart in the reference): times, on the
  * caller's DEVICE block of ns states (X in, HX overwritten), the launch shapes that leave
- * every bit of H|psi> unchanged -- stencil kernel (variants 2, 3, 4 of
+ * every bit of H|psi> unchanged -- stencil kernel (variants 2-5 of
  * qg_hamiltonian_set_stencil_kernel), states per projection block (2, 4, 8, 16) and per
  * scatter group (4, 8) -- one dimension at a time (the phases are independent), best of
  * three CUDA-event timed applies each, and keeps the fastest in the operator.

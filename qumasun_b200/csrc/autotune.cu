@@ -2,7 +2,8 @@
 //
 // Times, on the caller's own block of states, the launch shapes the engine can choose
 // without changing a single bit of the result: the stencil kernel (one-plane ring,
-// two-plane ring, two rows per thread; all give the same sums in the same order), the
+// two-plane ring, two rows per thread with V in the ring or from global memory; all give
+// the same sums in the same order), the
 // states per projection block (1-16) and the states per scatter group (4, 8). The split
 // of each atom's projector points over blocks is NOT tuned: it changes the summation
 // order, and results must not depend on the tuning or on the batch. Each phase is
@@ -53,7 +54,7 @@ int autotune(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, long lo
     // stencil kernel (phase 1)
     int best_v = 0;
     float best_t = FLT_MAX;
-    for (int v : {2, 3, 4}) {
+    for (int v : {2, 3, 4, 5}) {
         h->stencil_variant = v;
         const int rc = timed_phases<T>(h, ns, X, ldx, HX, ldhx, reps, ms);
         if (rc != QG_OK) {

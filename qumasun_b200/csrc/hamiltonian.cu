@@ -603,27 +603,29 @@ size_t coef_scratch_elems_z(qg_hamiltonian h, int nk, int nsk) {
 }
 
 // Stencil kernel for a real-state apply: the forced variant when it accepts the shape,
-// else the two-row ring kernel (4; measured on the 80^3 cell, 256 states: FP64 order 8
-// 0.553 ms against 0.764 for the one-plane kernel and 0.896 for the two-plane one, and
-// faster at every FP64 order and at FP32 orders 4-8), except FP32 order 2, where the
-// one-plane kernel (2) is faster (0.91 against 1.00 ms for the whole apply); then the
-// one-plane, then the two-plane ring kernel, else (1) the register-window kernel, which
-// takes any shape. All ring kernels give the same bits.
+// else the two-row ring kernel -- FP64 with V in the ring (4), FP32 with V from global
+// memory (5) -- measured on the 80^3 cell, 256 states (whole apply, order 2/4/6/8):
+// FP64 4: 1.46/1.52/1.52/1.55 ms, 5: 1.58/1.59/1.59/1.59, one-plane (2): 1.52/1.75/1.77/1.77;
+// FP32 5: 0.87/1.03/1.03/1.10, 4: 1.00/1.06/1.04/1.11, 2: 0.91/1.11/1.10/1.12;
+// then the other ring kernels, else (1) the register-window kernel, which takes any
+// shape. All ring kernels give the same bits.
 template <typename T>
 static int ring_stencil_variant(qg_hamiltonian h, const HamArgs<T>& a) {
     const int v = h->stencil_variant;
     if (v == 1) return 1;
     const bool pair_ok = stencil_pair_ok<T>(a, h->order);
     const bool tma_ok = stencil_tma_ok<T>(a, h->order);
-    const bool rows_ok = stencil_rows_ok<T>(a, h->order);
+    const bool rows_ok = stencil_rows_ok<T>(a, h->order, true);
+    const bool rowsg_ok = stencil_rows_ok<T>(a, h->order, false);
     if (v == 3 && pair_ok) return 3;
     if (v == 2 && tma_ok) return 2;
     if (v == 4 && rows_ok) return 4;
-    const bool one_plane_first = sizeof(T) == 4 && h->order == 2;
-    if (rows_ok && !(one_plane_first && tma_ok)) return 4;
+    if (v == 5 && rowsg_ok) return 5;
+    if (sizeof(T) == 4 && rowsg_ok) return 5;
+    if (rows_ok) return 4;
+    if (rowsg_ok) return 5;
     if (tma_ok) return 2;
     if (pair_ok) return 3;
-    if (rows_ok) return 4;
     return 1;
 }
 
@@ -682,7 +684,8 @@ int apply_hamiltonian(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX
     if (variant != 1) {
         auto stencil = [&]() {
             if (variant == 3) return launch_stencil_pair<T>(a, h->order, st);
-            if (variant == 4) return launch_stencil_rows<T>(a, h->order, st);
+            if (variant == 4) return launch_stencil_rows<T>(a, h->order, st, true);
+            if (variant == 5) return launch_stencil_rows<T>(a, h->order, st, false);
             return launch_stencil_tma<T>(a, h->order, st);
         };
         if (!nonlocal) {
@@ -1065,7 +1068,7 @@ int qg_hamiltonian_apply_timed_d(qg_hamiltonian h, int ns, const double* X, long
 }
 
 int qg_hamiltonian_set_stencil_kernel(qg_hamiltonian h, int variant) {
-    if (!h || variant < 0 || variant > 4) return QG_ERR_INVALID;
+    if (!h || variant < 0 || variant > 5) return QG_ERR_INVALID;
     h->stencil_variant = variant;
     return QG_OK;
 }

@@ -66,10 +66,11 @@ template <typename T>
 int launch_stencil_pair(const HamArgs<T>& a, int order, cudaStream_t st);
 template <typename T>
 bool stencil_pair_ok(const HamArgs<T>& a, int order);
-// Real states, two grid rows per consumer thread, V streamed through the ring (stencil_rows.cu).
+// Real states, two grid rows per consumer thread, V streamed through the ring (vring) or
+// read one plane ahead from global memory (stencil_rows.cu).
 template <typename T>
-int launch_stencil_rows(const HamArgs<T>& a, int order, cudaStream_t st);
+int launch_stencil_rows(const HamArgs<T>& a, int order, cudaStream_t st, bool vring = true);
 template <typename T>
-bool stencil_rows_ok(const HamArgs<T>& a, int order);
+bool stencil_rows_ok(const HamArgs<T>& a, int order, bool vring = true);
 
 }  // namespace qg

@@ -44,6 +44,10 @@ struct R16<double> {
         const double2 w = *reinterpret_cast<const double2*>(p);
         v[0] = w.x; v[1] = w.y;
     }
+    static __device__ __forceinline__ void ldg(double (&v)[2], const double* p) {
+        const double2 w = __ldg(reinterpret_cast<const double2*>(p));
+        v[0] = w.x; v[1] = w.y;
+    }
     static __device__ __forceinline__ void st(double* p, const double (&v)[2]) {
         *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
     }
@@ -52,6 +56,10 @@ template <>
 struct R16<float> {
     static __device__ __forceinline__ void ld(float (&v)[4], const float* p) {
         const float4 w = *reinterpret_cast<const float4*>(p);
+        v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+    }
+    static __device__ __forceinline__ void ldg(float (&v)[4], const float* p) {
+        const float4 w = __ldg(reinterpret_cast<const float4*>(p));
         v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
     }
     static __device__ __forceinline__ void st(float* p, const float (&v)[4]) {
@@ -85,7 +93,9 @@ __device__ __forceinline__ T lap_rows(T c, const T* xm, const T* xp, const T* ym
     }
 }
 
-template <typename T, int ORDER, int NXC>
+// VR: V rows streamed through the ring (true) or read from global memory one plane ahead
+// into registers (false: smaller stages, a deeper ring).
+template <typename T, int ORDER, int NXC, bool VR>
 __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<T> a, const WorkGrid wg, int nst) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = rows_radius<ORDER>();
@@ -101,7 +111,7 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
     const int nx = NXC > 0 ? NXC : a.nx, ny = a.ny, nz = a.nz, ty = a.ty;
     const int rows = ty + 2 * R;
     const int psi_elems = rows * nx;
-    const int stage_elems = psi_elems + ty * nx;  // psi rows, then the tile's V rows
+    const int stage_elems = psi_elems + (VR ? ty * nx : 0);  // psi rows, then (VR) the tile's V rows
     const int tpr = nx / PX;
     const int ncons = tpr * (ty / 2);
     const int ncons_warps = (ncons + 31) / 32;
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
     __syncthreads();
 
     if (t < 32) {
-        if (t == 0) produce_planes<T, R, 1, true>(a, wg, nst, nx, ringp, full, empty, ctl);
+        if (t == 0) produce_planes<T, R, 1, VR>(a, wg, nst, nx, ringp, full, empty, ctl);
     } else if (t < 32 + ncons) {
         const unsigned wmask = __activemask();
         const int lane = t & 31;
@@ -176,6 +186,12 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
             int jp = j;  // stage of plane z + R
             uint32_t php = ph;
             T* hcol = a.HX + state_offset(a, s, true) + col;
+            const T* vcol = a.V + col;
+            T vr0[PX], vr1[PX];  // !VR: V of plane z (rows ly0, ly0 + 1), loaded a step ahead
+            if constexpr (!VR) {
+                VV::ldg(vr0, vcol + (long long)zs * plane);
+                VV::ldg(vr1, vcol + (long long)zs * plane + nx);
+            }
             for (int z = zs; z < ze && !bad;) {
 #pragma unroll
                 for (int k = 0; k < Q; ++k) {
@@ -196,9 +212,21 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
                         VV::ld(ya[d - 1], st + cb0 - d * nx);
                         VV::ld(yb[d - 1], st + cb0 + (1 + d) * nx);
                     }
-                    T vv0[PX], vv1[PX];
-                    VV::ld(vv0, st + vb0);
-                    VV::ld(vv1, st + vb0 + nx);
+                    T vv0[PX], vv1[PX], vn0[PX], vn1[PX];
+                    if constexpr (VR) {
+                        VV::ld(vv0, st + vb0);
+                        VV::ld(vv1, st + vb0 + nx);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < PX; ++e) {
+                            vv0[e] = vr0[e];
+                            vv1[e] = vr1[e];
+                        }
+                        if (z + 1 < ze) {
+                            VV::ldg(vn0, vcol + (long long)(z + 1) * plane);
+                            VV::ldg(vn1, vcol + (long long)(z + 1) * plane + nx);
+                        }
+                    }
                     T out0[PX], out1[PX];
 #pragma unroll
                     for (int row = 0; row < 2; ++row) {
@@ -242,6 +270,15 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
                     if (lane == 0) mbar_arrive(&empty[jz]);  // plane z is no longer read
                     VV::st(hcol + (long long)z * plane, out0);
                     VV::st(hcol + (long long)z * plane + nx, out1);
+                    if constexpr (!VR) {
+                        if (z + 1 < ze) {
+#pragma unroll
+                            for (int e = 0; e < PX; ++e) {
+                                vr0[e] = vn0[e];
+                                vr1[e] = vn1[e];
+                            }
+                        }
+                    }
                     ++z;
                     if (++jz == nst) jz = 0;
                     if (++jp == nst) { jp = 0; php ^= 1u; }
@@ -271,34 +308,34 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_stencil_rows(const HamArgs<
 // Rows per tile: the largest even divisor of ny (<= 32) keeping the consumers (one per
 // PX x-points of a row pair) within the limit and the ring within its budget.
 template <typename T>
-int rows_tile(int nx, int ny, int R) {
+int rows_tile(int nx, int ny, int R, bool vr) {
     constexpr int PX = 16 / sizeof(T);
     int ty = 0;
     for (int t = 2; t <= 32; t += 2) {
         if (ny % t != 0 || (nx / PX) * (t / 2) > kRowsConsumers) continue;
-        const size_t stage = (size_t)(2 * t + 2 * R) * nx * sizeof(T);
+        const size_t stage = (size_t)((vr ? 2 * t : t) + 2 * R) * nx * sizeof(T);
         if (ring_stages(R, stage, 3, kRowsSmemKb) > 0) ty = t;
     }
     return ty;
 }
 
-template <typename T, int ORDER, int NXC = 0>
+template <typename T, int ORDER, bool VR, int NXC = 0>
 int launch_rows_order(const HamArgs<T>& a, cudaStream_t st) {
     constexpr int PX = 16 / sizeof(T);
     constexpr int R = rows_radius<ORDER>();
     if constexpr (NXC == 0) {
         switch (a.nx) {
-            case 40: return launch_rows_order<T, ORDER, 40>(a, st);
-            case 80: return launch_rows_order<T, ORDER, 80>(a, st);
-            case 120: return launch_rows_order<T, ORDER, 120>(a, st);
+            case 40: return launch_rows_order<T, ORDER, VR, 40>(a, st);
+            case 80: return launch_rows_order<T, ORDER, VR, 80>(a, st);
+            case 120: return launch_rows_order<T, ORDER, VR, 120>(a, st);
             default: break;
         }
     }
-    const size_t stage = (size_t)(2 * a.ty + 2 * R) * a.nx * sizeof(T);
+    const size_t stage = (size_t)((VR ? 2 * a.ty : a.ty) + 2 * R) * a.nx * sizeof(T);
     const int nst = ring_stages(R, stage, 3, kRowsSmemKb);
     if (nst < 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = kBarBytes + (size_t)nst * stage;
-    auto kern = k_stencil_rows<T, ORDER, NXC>;
+    auto kern = k_stencil_rows<T, ORDER, NXC, VR>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * (a.ty / 2);
@@ -324,7 +361,7 @@ int launch_rows_order(const HamArgs<T>& a, cudaStream_t st) {
 }  // namespace
 
 template <typename T>
-bool stencil_rows_ok(const HamArgs<T>& a, int order) {
+bool stencil_rows_ok(const HamArgs<T>& a, int order, bool vring) {
     constexpr int PX = 16 / sizeof(T);
     if (order != 2 && order != 4 && order != 6 && order != 8) return false;
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
@@ -332,27 +369,36 @@ bool stencil_rows_ok(const HamArgs<T>& a, int order) {
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R || a.nz < 2 * R)
         return false;
-    return rows_tile<T>(a.nx, a.ny, R) > 0;
+    return rows_tile<T>(a.nx, a.ny, R, vring) > 0;
 }
 
 template <typename T>
-int launch_stencil_rows(const HamArgs<T>& a, int order, cudaStream_t st) {
-    if (!stencil_rows_ok<T>(a, order)) return QG_ERR_UNSUPPORTED;
+int launch_stencil_rows(const HamArgs<T>& a, int order, cudaStream_t st, bool vring) {
+    if (!stencil_rows_ok<T>(a, order, vring)) return QG_ERR_UNSUPPORTED;
     HamArgs<T> b = a;
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
-    b.ty = rows_tile<T>(a.nx, a.ny, R);
+    b.ty = rows_tile<T>(a.nx, a.ny, R, vring);
+    if (vring) {
+        switch (order) {
+            case 2: return launch_rows_order<T, 2, true>(b, st);
+            case 4: return launch_rows_order<T, 4, true>(b, st);
+            case 6: return launch_rows_order<T, 6, true>(b, st);
+            case 8: return launch_rows_order<T, 8, true>(b, st);
+            default: return QG_ERR_INVALID;
+        }
+    }
     switch (order) {
-        case 2: return launch_rows_order<T, 2>(b, st);
-        case 4: return launch_rows_order<T, 4>(b, st);
-        case 6: return launch_rows_order<T, 6>(b, st);
-        case 8: return launch_rows_order<T, 8>(b, st);
+        case 2: return launch_rows_order<T, 2, false>(b, st);
+        case 4: return launch_rows_order<T, 4, false>(b, st);
+        case 6: return launch_rows_order<T, 6, false>(b, st);
+        case 8: return launch_rows_order<T, 8, false>(b, st);
         default: return QG_ERR_INVALID;
     }
 }
 
-template bool stencil_rows_ok<double>(const HamArgs<double>&, int);
-template bool stencil_rows_ok<float>(const HamArgs<float>&, int);
-template int launch_stencil_rows<double>(const HamArgs<double>&, int, cudaStream_t);
-template int launch_stencil_rows<float>(const HamArgs<float>&, int, cudaStream_t);
+template bool stencil_rows_ok<double>(const HamArgs<double>&, int, bool);
+template bool stencil_rows_ok<float>(const HamArgs<float>&, int, bool);
+template int launch_stencil_rows<double>(const HamArgs<double>&, int, cudaStream_t, bool);
+template int launch_stencil_rows<float>(const HamArgs<float>&, int, cudaStream_t, bool);
 
 }  // namespace qg

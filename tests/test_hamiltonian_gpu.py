@@ -229,7 +229,7 @@ def test_every_stencil_kernel_agrees_with_oracle(cuda_ctx, grid, order):
     ref = O.hamiltonian_apply(cell, X, fd_order=order)
     H = Hamiltonian(cuda_ctx, cell, fd_order=order)
     ring = {}
-    for variant in (0, 1, 2, 3, 4):
+    for variant in (0, 1, 2, 3, 4, 5):
         H.set_stencil_kernel(variant)
         for dt, tol in ((torch.float64, TOL64), (torch.float32, TOL32)):
             out = H.apply(torch.from_numpy(X).to("cuda", dt))
@@ -258,7 +258,7 @@ def test_autotuner_keeps_the_bits(cuda_ctx):
     for Xd in (X, X.float()):
         before = H.apply(Xd).cpu().numpy()
         ch = H.autotune(Xd)
-        assert ch["stencil"] in (2, 3, 4) and ch["project_states"] in (2, 4, 8, 16)
+        assert ch["stencil"] in (2, 3, 4, 5) and ch["project_states"] in (2, 4, 8, 16)
         assert ch["scatter_states"] in (4, 8) and all(v > 0 for v in ch["ms_phases"])
         np.testing.assert_array_equal(H.apply(Xd).cpu().numpy(), before)
     assert cuda_ctx.take_device_status() == 0
