@@ -138,7 +138,9 @@ int qg_hamiltonian_apply_host_d(qg_hamiltonian ham, int ns, const double* X, dou
  * reference's {re[N], im[N]} state layout (lobpcg_z_multi_mpi.h:1005-1012).
  * g is the operator's Bloch vector (descriptor or qg_hamiltonian_set_kvector);
  * the projectors carry exp(i g.r) at the unwrapped image position of each
- * cube point. FD order 8 only (KINETIC_8TH; other orders QG_ERR_UNSUPPORTED).
+ * cube point. FD order 8, 6 or 2 (KINETIC_8TH / _6TH / _2ND of qumasun_kpoint.matrix.h:78-86:
+ * LaplasianKpoint8th/6th/2nd); order 4 returns QG_ERR_UNSUPPORTED (the reference has no
+ * 4th-order k-point stencil).
  * Replaces OpeA(SoAComplex& Ax, const SoAComplex& x) of qumasun_kpoint.lobpcg.h:38-40
  * -> QUMASUN_KPOINT::mHamiltonianMatrix_ddm (qumasun_kpoint.matrix.h:25-50):
  * mPotentialMatrix_ddm on re and im, PseudoPotIntegrator_kpoint::ProjectionPP
@@ -462,7 +464,7 @@ int qg_potential_lda_d(qg_poisson p, const double* rho, const double* pcc, const
 
 /* One fourth-order Taylor step psi <- sum_{j=0..4} (-i dt H)^j / j! psi of ns complex
  * {re[N], im[N]} states (DEVICE, in place, ldx >= 2N) under the operator at its
- * k-vector (FD order 8): four applications of H to the whole block, each followed by
+ * k-vector (FD order 2, 6 or 8): four applications of H to the whole block, each followed by
  * the update of that order. Work: two blocks of ns states kept by the operator.
  * Replaces QUMASUN::TimeEvoH4 (qumasun_td.time_evo_H4.h:13-60), which steps one state
  * at a time. */

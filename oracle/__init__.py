@@ -97,6 +97,7 @@ def port_lib():
                                              C.c_double, C.c_double, C.c_double, C.c_double,
                                              C.c_double, _dp, _dp, _dp, _dp]
         lib.or_hamiltonian_apply.argtypes = [C.POINTER(HamDescC), C.c_int, _dp, _dp]
+        lib.or_laplacian_kpoint.argtypes = [C.c_int] * 4 + [C.c_double] * 7 + [_dp] * 4
         lib.or_hamiltonian_kpoint_local.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
                                                     C.c_double, C.c_int, _dp, _dp]
         lib.or_hamiltonian_kpoint_apply.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
@@ -121,6 +122,7 @@ def ref_lib():
                                               C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.c_double, _dp, _dp, _dp, _dp]
         lib.ref_hamiltonian_apply.argtypes = [C.POINTER(HamDescC), C.c_int, _dp, _dp]
+        lib.ref_laplacian_kpoint.argtypes = [C.c_int] * 4 + [C.c_double] * 7 + [_dp] * 4
         lib.ref_lobpcg_d_multi.argtypes = [C.POINTER(HamDescC), C.c_int, C.c_int, _dp, _dp, _dp,
                                            C.c_int, C.c_int, _ip]
         lib.ref_grid_for_sphere.argtypes = [C.c_double] * 7 + [_ip]
@@ -157,6 +159,20 @@ def laplacian(order, grid, h, coef, psi, impl="port"):
     if rc != 0:
         raise ValueError(f"laplacian order {order} rejected ({rc})")
     return out
+
+
+def laplacian_kpoint(order, grid, h, coef, g, re, im, impl="port"):
+    """(out_re, out_im) += coef (Lap + 2i g.grad - g^2) on split re/im arrays, FD order 2,
+    6 or 8 (LaplasianKpoint{2nd,6th,8th}_halo)."""
+    lib = port_lib() if impl == "port" else ref_lib()
+    fn = lib.or_laplacian_kpoint if impl == "port" else lib.ref_laplacian_kpoint
+    re, im = _c64(re), _c64(im)
+    ore, oim = np.zeros_like(re), np.zeros_like(im)
+    rc = fn(order, grid[0], grid[1], grid[2], h[0], h[1], h[2], coef, g[0], g[1], g[2], _ptr(re, _dp), _ptr(im, _dp),
+            _ptr(ore, _dp), _ptr(oim, _dp))
+    if rc != 0:
+        raise ValueError(f"laplacian_kpoint rejected order {order}")
+    return ore, oim
 
 
 def laplacian_kpoint8(grid, h, coef, g, re, im, impl="port"):
@@ -196,12 +212,12 @@ def hamiltonian_kpoint_local(cell, g, X):
     return HX
 
 
-def hamiltonian_kpoint_apply(cell, g, X, impl="port"):
+def hamiltonian_kpoint_apply(cell, g, X, impl="port", fd_order=8):
     """Complex k-point H (V + nonlocal with Bloch phases + 8th-order k-point kinetic)
     on {re, im} states X (ns, 2N); g = Bloch vector in bohr^-1."""
     X = _c64(X)
     HX = np.zeros_like(X)
-    desc = HamDesc(cell, 8)
+    desc = HamDesc(cell, fd_order)
     if impl == "port":
         rc = port_lib().or_hamiltonian_kpoint_apply(C.byref(desc.c), g[0], g[1], g[2], X.shape[0],
                                                     _ptr(X, _dp), _ptr(HX, _dp))

@@ -157,7 +157,88 @@ static void kpoint8_pass(int nx, int ny, int nz, double hx, double hy, double hz
                 if (KX || KY || KZ) out2[io] += g;
             }
 }
+/* The 6th-order pass of LaplasianKpoint6th_halo_f (GridDifferenceKpoint6th.h:19-107):
+ * c0 = -245 coef sum 1/(90 h^2) - coef g^2, second-derivative (1, -13.5, 135)/(90 h^2),
+ * first derivative (45, -9, 1)/(60 h). */
+static void kpoint6_pass(int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                         double sign1st, double gx, double gy, double gz, const double* in,
+                         double* out, double* out2) {
+    const int KX = fabs(gx) >= 1.0e-8, KY = fabs(gy) >= 1.0e-8, KZ = fabs(gz) >= 1.0e-8;
+    const double c0 = -245.0 * coef * (1.0 / (90.0 * hx * hx) + 1.0 / (90.0 * hy * hy) + 1.0 / (90.0 * hz * hz)) - coef * (gx * gx + gy * gy + gz * gz);
+    const double c3x = coef / (90.0 * hx * hx), c2x = -13.5 * coef / (90.0 * hx * hx), c1x = 135.0 * coef / (90.0 * hx * hx);
+    const double c3y = coef / (90.0 * hy * hy), c2y = -13.5 * coef / (90.0 * hy * hy), c1y = 135.0 * coef / (90.0 * hy * hy);
+    const double c3z = coef / (90.0 * hz * hz), c2z = -13.5 * coef / (90.0 * hz * hz), c1z = 135.0 * coef / (90.0 * hz * hz);
+    const double coef2 = sign1st * coef * 2.0;
+    const double a1x = 45.0 * coef2 * gx / (60.0 * hx), a2x = -9.0 * coef2 * gx / (60.0 * hx), a3x = coef2 * gx / (60.0 * hx);
+    const double a1y = 45.0 * coef2 * gy / (60.0 * hy), a2y = -9.0 * coef2 * gy / (60.0 * hy), a3y = coef2 * gy / (60.0 * hy);
+    const double a1z = 45.0 * coef2 * gz / (60.0 * hz), a2z = -9.0 * coef2 * gz / (60.0 * hz), a3z = coef2 * gz / (60.0 * hz);
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                const size_t io = ix + (size_t)nx * (iy + (size_t)ny * iz);
+                double d = c0 * P(0, 0, 0);
+                d += c3x * (P(3, 0, 0) + P(-3, 0, 0)) + c2x * (P(2, 0, 0) + P(-2, 0, 0)) + c1x * (P(1, 0, 0) + P(-1, 0, 0));
+                d += c3y * (P(0, 3, 0) + P(0, -3, 0)) + c2y * (P(0, 2, 0) + P(0, -2, 0)) + c1y * (P(0, 1, 0) + P(0, -1, 0));
+                d += c3z * (P(0, 0, 3) + P(0, 0, -3)) + c2z * (P(0, 0, 2) + P(0, 0, -2)) + c1z * (P(0, 0, 1) + P(0, 0, -1));
+                out[io] += d;
+                double g = 0.0;
+                if (KX) g += a3x * (P(3, 0, 0) - P(-3, 0, 0)) + a2x * (P(2, 0, 0) - P(-2, 0, 0)) + a1x * (P(1, 0, 0) - P(-1, 0, 0));
+                if (KY) g += a3y * (P(0, 3, 0) - P(0, -3, 0)) + a2y * (P(0, 2, 0) - P(0, -2, 0)) + a1y * (P(0, 1, 0) - P(0, -1, 0));
+                if (KZ) g += a3z * (P(0, 0, 3) - P(0, 0, -3)) + a2z * (P(0, 0, 2) - P(0, 0, -2)) + a1z * (P(0, 0, 1) - P(0, 0, -1));
+                if (KX || KY || KZ) out2[io] += g;
+            }
+}
+
+/* The 2nd-order pass of LaplasianKpoint2nd_halo_f (GridDifferenceKpoint2nd.h:19-92):
+ * d = c0 p + c1x (p+x + p-x) + c1y (..) + c1z (..), c0 = -coef sum 2/h^2 - coef g^2,
+ * first derivative coef2 g / (2h). */
+static void kpoint2_pass(int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                         double sign1st, double gx, double gy, double gz, const double* in,
+                         double* out, double* out2) {
+    const int KX = fabs(gx) >= 1.0e-8, KY = fabs(gy) >= 1.0e-8, KZ = fabs(gz) >= 1.0e-8;
+    const double c0 = -coef * (2.0 / (hx * hx) + 2.0 / (hy * hy) + 2.0 / (hz * hz)) - coef * (gx * gx + gy * gy + gz * gz);
+    const double c1x = coef / (hx * hx), c1y = coef / (hy * hy), c1z = coef / (hz * hz);
+    const double coef2 = sign1st * coef * 2.0;
+    const double a1x = coef2 * gx / (2.0 * hx), a1y = coef2 * gy / (2.0 * hy), a1z = coef2 * gz / (2.0 * hz);
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                const size_t io = ix + (size_t)nx * (iy + (size_t)ny * iz);
+                const double d = c0 * P(0, 0, 0) + c1x * (P(1, 0, 0) + P(-1, 0, 0)) + c1y * (P(0, 1, 0) + P(0, -1, 0)) +
+                                 c1z * (P(0, 0, 1) + P(0, 0, -1));
+                out[io] += d;
+                double g = 0.0;
+                if (KX) g += a1x * (P(1, 0, 0) - P(-1, 0, 0));
+                if (KY) g += a1y * (P(0, 1, 0) - P(0, -1, 0));
+                if (KZ) g += a1z * (P(0, 0, 1) - P(0, 0, -1));
+                if (KX || KY || KZ) out2[io] += g;
+            }
+}
 #undef P
+
+/* LaplasianKpoint{2nd,6th,8th}_halo (GridDifferenceKpoint2nd.h, 6th.h:109-142,
+ * 8th.h:124-157) for order 2, 6 or 8: the real part pass (sign +1) writes out_re and the
+ * first-derivative term into out_im, the imaginary part pass (sign -1) writes out_im
+ * and the derivative into out_re. Returns -1 for another order. */
+int or_laplacian_kpoint(int order, int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                        double gx, double gy, double gz, const double* re, const double* im,
+                        double* out_re, double* out_im) {
+    switch (order) {
+        case 2:
+            kpoint2_pass(nx, ny, nz, hx, hy, hz, coef, +1.0, gx, gy, gz, re, out_re, out_im);
+            kpoint2_pass(nx, ny, nz, hx, hy, hz, coef, -1.0, gx, gy, gz, im, out_im, out_re);
+            return 0;
+        case 6:
+            kpoint6_pass(nx, ny, nz, hx, hy, hz, coef, +1.0, gx, gy, gz, re, out_re, out_im);
+            kpoint6_pass(nx, ny, nz, hx, hy, hz, coef, -1.0, gx, gy, gz, im, out_im, out_re);
+            return 0;
+        case 8:
+            kpoint8_pass(nx, ny, nz, hx, hy, hz, coef, +1.0, gx, gy, gz, re, out_re, out_im);
+            kpoint8_pass(nx, ny, nz, hx, hy, hz, coef, -1.0, gx, gy, gz, im, out_im, out_re);
+            return 0;
+        default: return -1;
+    }
+}
 
 /* LaplasianKpoint8th_halo (GridDifferenceKpoint8th.h:124-157): the real part
  * pass (sign +1) writes out_re and the first-derivative term into out_im, the
@@ -246,7 +327,9 @@ int or_hamiltonian_kpoint_local(const or_ham_desc* d, double gx, double gy, doub
         double* ore = HX + (size_t)s * 2 * N;
         double* oim = ore + N;
         for (size_t i = 0; i < N; ++i) { ore[i] = d->V[i] * re[i]; oim[i] = d->V[i] * im[i]; }
-        or_laplacian_kpoint8(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, gx, gy, gz, re, im, ore, oim);
+        if (or_laplacian_kpoint(d->fd_order, d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, gx, gy, gz, re, im, ore,
+                                oim) != 0)
+            return -1;
     }
     return 0;
 }
@@ -307,7 +390,7 @@ static void nonlocal_kpoint_one(const or_ham_desc* d, double gx, double gy, doub
 
 /* Complex k-point Hamiltonian, mHamiltonianMatrix_ddm of QUMASUN_KPOINT
  * (qumasun_kpoint.matrix.h:25-50): V on re and im, the k-point nonlocal term,
- * then the 8th-order k-point kinetic term. Each state is {re[N], im[N]} contiguous. */
+ * then the k-point kinetic term of the descriptor's FD order (2, 6 or 8). Each state is {re[N], im[N]} contiguous. */
 int or_hamiltonian_kpoint_apply(const or_ham_desc* d, double gx, double gy, double gz, int ns, const double* X,
                                 double* HX) {
     const size_t N = (size_t)d->nx * d->ny * d->nz;
@@ -318,7 +401,9 @@ int or_hamiltonian_kpoint_apply(const or_ham_desc* d, double gx, double gy, doub
         double* oim = ore + N;
         for (size_t i = 0; i < N; ++i) { ore[i] = d->V[i] * re[i]; oim[i] = d->V[i] * im[i]; }
         if (d->n_atoms > 0 && d->n_proj > 0) nonlocal_kpoint_one(d, gx, gy, gz, re, im, ore, oim);
-        or_laplacian_kpoint8(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, gx, gy, gz, re, im, ore, oim);
+        if (or_laplacian_kpoint(d->fd_order, d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, gx, gy, gz, re, im, ore,
+                                oim) != 0)
+            return -1;
     }
     return 0;
 }

@@ -52,6 +52,8 @@
 #include "GridDifference6th.h"
 #include "GridDifference8th.h"
 #include "GridDifferenceKpoint8th.h"
+#include "GridDifferenceKpoint2nd.h"
+#include "GridDifferenceKpoint6th.h"
 #include "w_dsygvx.h"
 
 /* lobpcg_d_multi.h:209 and :284 call lapack_DSYGVX with six arguments while
@@ -186,6 +188,36 @@ int ref_laplacian_kpoint8(int nx, int ny, int nz, double hx, double hy, double h
     case A * 4 + B * 2 + C:                                                                   \
         LaplasianKpoint8th_halo<A, B, C>(grid, out, src, bre.data(), bim.data(), coef, hx, hy, hz, \
                                          gx, gy, gz);                                         \
+        break;
+    switch (sel) {
+        QG_KP(0, 0, 0) QG_KP(0, 0, 1) QG_KP(0, 1, 0) QG_KP(0, 1, 1)
+        QG_KP(1, 0, 0) QG_KP(1, 0, 1) QG_KP(1, 1, 0) QG_KP(1, 1, 1)
+    }
+#undef QG_KP
+    return 0;
+}
+
+/* The same for FD order 2 (LaplasianKpoint2nd_halo, GridDifferenceKpoint2nd.h:97-130), 6
+ * (LaplasianKpoint6th_halo, GridDifferenceKpoint6th.h:108-142) or 8. */
+int ref_laplacian_kpoint(int order, int nx, int ny, int nz, double hx, double hy, double hz, double coef,
+                         double gx, double gy, double gz, const double* re, const double* im,
+                         double* out_re, double* out_im) {
+    if (order == 8) return ref_laplacian_kpoint8(nx, ny, nz, hx, hy, hz, coef, gx, gy, gz, re, im, out_re, out_im);
+    if (order != 2 && order != 6) return -1;
+    GridRange grid{0, 0, 0, nx, ny, nz};
+    std::vector<double> bre((size_t)(nx + 8) * (ny + 8) * (nz + 8));
+    std::vector<double> bim(bre.size());
+    SoAComplex out{out_re, out_im};
+    SoAComplex src{const_cast<double*>(re), const_cast<double*>(im)};
+    const double th = 1.0e-8;
+    const int kx = fabs(gx) >= th, ky = fabs(gy) >= th, kz = fabs(gz) >= th;
+    const int sel = kx * 4 + ky * 2 + kz;
+#define QG_KP(A, B, C)                                                                                     \
+    case A * 4 + B * 2 + C:                                                                                \
+        if (order == 2)                                                                                    \
+            LaplasianKpoint2nd_halo<A, B, C>(grid, out, src, bre.data(), bim.data(), coef, hx, hy, hz, gx, gy, gz); \
+        else                                                                                               \
+            LaplasianKpoint6th_halo<A, B, C>(grid, out, src, bre.data(), bim.data(), coef, hx, hy, hz, gx, gy, gz); \
         break;
     switch (sel) {
         QG_KP(0, 0, 0) QG_KP(0, 0, 1) QG_KP(0, 1, 0) QG_KP(0, 1, 1)
@@ -459,7 +491,8 @@ struct RefKpointHamiltonian {
             SoAComplex ps{const_cast<double*>(re), const_cast<double*>(im)};
             pp.ProjectionPP(hp, ps, grid, nuclei.data(), d->n_atoms, 0);
         }
-        ref_laplacian_kpoint8(d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, g[0], g[1], g[2], re, im, ore, oim);
+        ref_laplacian_kpoint(d->fd_order, d->nx, d->ny, d->nz, d->hx, d->hy, d->hz, -0.5, g[0], g[1], g[2], re, im,
+                             ore, oim);
     }
 };
 
@@ -472,7 +505,7 @@ extern "C" {
  * the cubes in d. Returns -2 if a cube differs from GridForSphere(R, rc). */
 int ref_hamiltonian_kpoint_apply(const ref_ham_desc* d, double gx, double gy, double gz, double rc, int ns,
                                  const double* X, double* HX) {
-    if (d->fd_order != 8) return -1;
+    if (d->fd_order != 2 && d->fd_order != 6 && d->fd_order != 8) return -1;
     RefKpointHamiltonian H(d, gx, gy, gz, rc);
     if (H.status) return H.status;
     const size_t N = (size_t)d->nx * d->ny * d->nz;

@@ -476,12 +476,12 @@ int TcGram::gram(cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, 
     if (pieces == 2) {
         auto kern = k_gram_tc<2, stages<2>()>;
         const size_t sm = smem_bytes<2>();
-        QG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        QG_CUDA_TRY(allow_max_dynamic_smem(kern));
         kern<<<grid, kThreads, sm, st>>>(tm, u, part.as<double>(), err);
     } else {
         auto kern = k_gram_tc<3, stages<3>()>;
         const size_t sm = smem_bytes<3>();
-        QG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        QG_CUDA_TRY(allow_max_dynamic_smem(kern));
         kern<<<grid, kThreads, sm, st>>>(tm, u, part.as<double>(), err);
     }
     QG_CUDA_TRY(cudaGetLastError());

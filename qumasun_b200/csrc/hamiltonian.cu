@@ -396,7 +396,7 @@ static int launch_project_nch(const DevProjectors& pj, const T* tab, int ns, con
     do {                                                                                                       \
         const size_t smem = (size_t)kProjDepth * (SBV + NCH) * kProjThreads * sizeof(T);                       \
         auto kern = k_project<T, SBV, NCH, kProjDepth>;                                                        \
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) \
+        if (allow_max_dynamic_smem(kern) != cudaSuccess) \
             return QG_ERR_CUDA;                                                                                \
         e = launch_clustered(kern, g, dim3(kProjThreads), parts, smem, st, X, ldx, ns, pj.atom_off, pj.pt_g,   \
                              tab, pj.npts, scale, coef, ldc, parts);                                           \
@@ -582,7 +582,7 @@ static int launch_stencil(const HamArgs<T>& a, int nz, cudaStream_t st) {
     const size_t smem = (size_t)SPB * (a.ty + 2 * R) * (a.nx + 2 * R) * sizeof(T);
     auto kern = k_hamiltonian<T, ORDER, SPB>;
     if (smem > 48 * 1024) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        if (allow_max_dynamic_smem(kern) != cudaSuccess)
             return QG_ERR_UNSUPPORTED;
     }
     dim3 grid(tiles, sgroups, nslab);

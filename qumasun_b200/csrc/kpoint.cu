@@ -232,10 +232,13 @@ __global__ void __launch_bounds__(256, 2) k_scatter_all_z(T* __restrict__ HX, lo
     }
 }
 
-// Any-shape fallback for V u - 1/2 (Lap + 2i g.grad - g^2) u: one thread per
-// (point, state), neighbours read from global memory with periodic wrap.
-template <typename T>
+// Any-shape fallback for V u - 1/2 (Lap + 2i g.grad - g^2) u at FD order 2, 6 or 8: one
+// thread per (point, state), neighbours read from global memory with periodic wrap. The
+// sums follow LaplasianKpoint{2nd,6th,8th}_halo_f (order 2: c0 p + cx (p+x + p-x) + ...;
+// orders 6, 8: c0 p, then the x, y and z groups).
+template <typename T, int ORDER>
 __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<T> a) {
+    constexpr int R = ORDER == 2 ? 1 : (ORDER == 6 ? 3 : 4);
     const long long N = (long long)a.nx * a.ny * a.nz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -262,21 +265,37 @@ __global__ void __launch_bounds__(256) k_kpoint_plain(const HamArgs<T> a) {
         auto at = [&](int dx, int dy, int dz) {
             return u[wrap_idx(ix + dx, a.nx) + (long long)a.nx * (wrap_idx(iy + dy, a.ny) + (long long)a.ny * wrap_idx(iz + dz, a.nz))];
         };
-        T xm[4], xp[4], ym[4], yp[4], zm[4], zp[4];
-        for (int d = 1; d <= 4; ++d) {
+        T xm[R], xp[R], ym[R], yp[R], zm[R], zp[R];
+        for (int d = 1; d <= R; ++d) {
             xm[d - 1] = at(-d, 0, 0); xp[d - 1] = at(d, 0, 0);
             ym[d - 1] = at(0, -d, 0); yp[d - 1] = at(0, d, 0);
             zm[d - 1] = at(0, 0, -d); zp[d - 1] = at(0, 0, d);
         }
         cen[c] = u[i];
-        T l = c0 * cen[c];
-        l += a.cx[3] * (xp[3] + xm[3]) + a.cx[2] * (xp[2] + xm[2]) + a.cx[1] * (xp[1] + xm[1]) + a.cx[0] * (xp[0] + xm[0]);
-        l += a.cy[3] * (yp[3] + ym[3]) + a.cy[2] * (yp[2] + ym[2]) + a.cy[1] * (yp[1] + ym[1]) + a.cy[0] * (yp[0] + ym[0]);
-        l += a.cz[3] * (zp[3] + zm[3]) + a.cz[2] * (zp[2] + zm[2]) + a.cz[1] * (zp[1] + zm[1]) + a.cz[0] * (zp[0] + zm[0]);
+        T l, g;
+        if constexpr (ORDER == 2) {
+            l = c0 * cen[c] + a.cx[0] * (xp[0] + xm[0]) + a.cy[0] * (yp[0] + ym[0]) + a.cz[0] * (zp[0] + zm[0]);
+            g = dxc[0] * (xp[0] - xm[0]);
+            g += dyc[0] * (yp[0] - ym[0]);
+            g += dzc[0] * (zp[0] - zm[0]);
+        } else if constexpr (ORDER == 6) {
+            l = c0 * cen[c];
+            l += a.cx[2] * (xp[2] + xm[2]) + a.cx[1] * (xp[1] + xm[1]) + a.cx[0] * (xp[0] + xm[0]);
+            l += a.cy[2] * (yp[2] + ym[2]) + a.cy[1] * (yp[1] + ym[1]) + a.cy[0] * (yp[0] + ym[0]);
+            l += a.cz[2] * (zp[2] + zm[2]) + a.cz[1] * (zp[1] + zm[1]) + a.cz[0] * (zp[0] + zm[0]);
+            g = dxc[2] * (xp[2] - xm[2]) + dxc[1] * (xp[1] - xm[1]) + dxc[0] * (xp[0] - xm[0]);
+            g += dyc[2] * (yp[2] - ym[2]) + dyc[1] * (yp[1] - ym[1]) + dyc[0] * (yp[0] - ym[0]);
+            g += dzc[2] * (zp[2] - zm[2]) + dzc[1] * (zp[1] - zm[1]) + dzc[0] * (zp[0] - zm[0]);
+        } else {
+            l = c0 * cen[c];
+            l += a.cx[3] * (xp[3] + xm[3]) + a.cx[2] * (xp[2] + xm[2]) + a.cx[1] * (xp[1] + xm[1]) + a.cx[0] * (xp[0] + xm[0]);
+            l += a.cy[3] * (yp[3] + ym[3]) + a.cy[2] * (yp[2] + ym[2]) + a.cy[1] * (yp[1] + ym[1]) + a.cy[0] * (yp[0] + ym[0]);
+            l += a.cz[3] * (zp[3] + zm[3]) + a.cz[2] * (zp[2] + zm[2]) + a.cz[1] * (zp[1] + zm[1]) + a.cz[0] * (zp[0] + zm[0]);
+            g = dxc[3] * (xp[3] - xm[3]) + dxc[2] * (xp[2] - xm[2]) + dxc[1] * (xp[1] - xm[1]) + dxc[0] * (xp[0] - xm[0]);
+            g += dyc[3] * (yp[3] - ym[3]) + dyc[2] * (yp[2] - ym[2]) + dyc[1] * (yp[1] - ym[1]) + dyc[0] * (yp[0] - ym[0]);
+            g += dzc[3] * (zp[3] - zm[3]) + dzc[2] * (zp[2] - zm[2]) + dzc[1] * (zp[1] - zm[1]) + dzc[0] * (zp[0] - zm[0]);
+        }
         lap[c] = l;
-        T g = dxc[3] * (xp[3] - xm[3]) + dxc[2] * (xp[2] - xm[2]) + dxc[1] * (xp[1] - xm[1]) + dxc[0] * (xp[0] - xm[0]);
-        g += dyc[3] * (yp[3] - ym[3]) + dyc[2] * (yp[2] - ym[2]) + dyc[1] * (yp[1] - ym[1]) + dyc[0] * (yp[0] - ym[0]);
-        g += dzc[3] * (zp[3] - zm[3]) + dzc[2] * (zp[2] - zm[2]) + dzc[1] * (zp[1] - zm[1]) + dzc[0] * (zp[0] - zm[0]);
         der[c] = g;
     }
     const T v = a.V[i];
@@ -373,21 +392,41 @@ int ensure_bloch_tables(qg_hamiltonian h, int nk, const double* kv, cudaStream_t
     return QG_OK;
 }
 
-// c0 and the first-derivative coefficients of -1/2 (Lap + 2i g.grad - g^2), exactly as
-// LaplasianKpoint8th_halo_f forms them: out[0] = c0, out[1..4] = dx, [5..8] = dy, [9..12] = dz
+// c0 and the first-derivative coefficients of -1/2 (Lap + 2i g.grad - g^2) at FD order
+// 2, 6 or 8, exactly as LaplasianKpoint{2nd,6th,8th}_halo_f form them
+// (GridDifferenceKpoint2nd.h:19-35, 6th.h:19-47, 8th.h:18-50): out[0] = c0,
+// out[1..4] = dx, [5..8] = dy, [9..12] = dz (first R entries of each used).
 void kpoint_coefs(const qg_hamiltonian h, const double* g, double* out) {
     const double coefk = -0.5;
     const double hh[3] = {h->hx, h->hy, h->hz};
-    out[0] = -14350.0 / 5040.0 * coefk * (1.0 / (hh[0] * hh[0]) + 1.0 / (hh[1] * hh[1]) + 1.0 / (hh[2] * hh[2])) -
-             coefk * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    const double gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    if (h->order == 2)
+        out[0] = -coefk * (2.0 / (hh[0] * hh[0]) + 2.0 / (hh[1] * hh[1]) + 2.0 / (hh[2] * hh[2])) - coefk * gg;
+    else if (h->order == 6)
+        out[0] = -245.0 * coefk *
+                     (1.0 / (90.0 * hh[0] * hh[0]) + 1.0 / (90.0 * hh[1] * hh[1]) + 1.0 / (90.0 * hh[2] * hh[2])) -
+                 coefk * gg;
+    else
+        out[0] = -14350.0 / 5040.0 * coefk * (1.0 / (hh[0] * hh[0]) + 1.0 / (hh[1] * hh[1]) + 1.0 / (hh[2] * hh[2])) -
+                 coefk * gg;
     const double coef2 = coefk * 2.0;
     for (int d = 0; d < 3; ++d) {
-        const bool on = std::fabs(g[d]) >= 1.0e-8;  // LaplasianKpoint8th_ddm skips |g| < 1e-8
+        const bool on = std::fabs(g[d]) >= 1.0e-8;  // the reference's _ddm skips |g| < 1e-8
         double* o = out + 1 + 4 * d;
-        o[0] = on ? 672.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
-        o[1] = on ? -168.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
-        o[2] = on ? 32.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
-        o[3] = on ? -3.0 * coef2 * g[d] / (840.0 * hh[d]) : 0.0;
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+        if (!on) continue;
+        if (h->order == 2) {
+            o[0] = coef2 * g[d] / (2.0 * hh[d]);
+        } else if (h->order == 6) {
+            o[0] = 45.0 * coef2 * g[d] / (60.0 * hh[d]);
+            o[1] = -9.0 * coef2 * g[d] / (60.0 * hh[d]);
+            o[2] = coef2 * g[d] / (60.0 * hh[d]);
+        } else {
+            o[0] = 672.0 * coef2 * g[d] / (840.0 * hh[d]);
+            o[1] = -168.0 * coef2 * g[d] / (840.0 * hh[d]);
+            o[2] = 32.0 * coef2 * g[d] / (840.0 * hh[d]);
+            o[3] = -3.0 * coef2 * g[d] / (840.0 * hh[d]);
+        }
     }
 }
 
@@ -397,7 +436,7 @@ template <typename T>
 int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, const T* X, long long ldx,
                          long long ldk, T* HX, long long ldhx, long long ldkh, T* coef, cudaStream_t st,
                          PhaseTimer* pt) {
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     const DevProjectors& pj = h->pj;
     const long long N = h->N();
     HamArgs<T> a{};
@@ -411,11 +450,20 @@ int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, co
     const double hh[3] = {h->hx, h->hy, h->hz};
     T* cs[3] = {a.cx, a.cy, a.cz};
     for (int d = 0; d < 3; ++d) {
-        const double s = 5040.0 * hh[d] * hh[d];
-        cs[d][3] = T(-9.0 * coefk / s);
-        cs[d][2] = T(128.0 * coefk / s);
-        cs[d][1] = T(-1008.0 * coefk / s);
-        cs[d][0] = T(8064.0 * coefk / s);
+        if (h->order == 2) {
+            cs[d][0] = T(coefk / (hh[d] * hh[d]));
+        } else if (h->order == 6) {
+            const double s = 90.0 * hh[d] * hh[d];
+            cs[d][2] = T(coefk / s);
+            cs[d][1] = T(-13.5 * coefk / s);
+            cs[d][0] = T(135.0 * coefk / s);
+        } else {
+            const double s = 5040.0 * hh[d] * hh[d];
+            cs[d][3] = T(-9.0 * coefk / s);
+            cs[d][2] = T(128.0 * coefk / s);
+            cs[d][1] = T(-1008.0 * coefk / s);
+            cs[d][0] = T(8064.0 * coefk / s);
+        }
     }
     std::vector<double> kc((size_t)13 * nk);
     for (int k = 0; k < nk; ++k) kpoint_coefs(h, kv + 3 * k, kc.data() + 13 * k);
@@ -467,11 +515,15 @@ int apply_hamiltonian_zk(qg_hamiltonian h, int nk, const double* kv, int nsk, co
     }
     if (pt) pt->mark(1, st);
     constexpr int PX = 16 / sizeof(T);
-    if (h->stencil_variant == 1 || !stencil_tma_ok<T>(a, 8, 2) || (nk > 1 && (ldk % PX || ldkh % PX))) {
+    if (h->stencil_variant == 1 || !stencil_tma_ok<T>(a, h->order, 2) || (nk > 1 && (ldk % PX || ldkh % PX))) {
         dim3 g((unsigned)((N + 255) / 256), (unsigned)(nk * nsk));
-        k_kpoint_plain<T><<<g, 256, 0, st>>>(a);
+        switch (h->order) {
+            case 2: k_kpoint_plain<T, 2><<<g, 256, 0, st>>>(a); break;
+            case 6: k_kpoint_plain<T, 6><<<g, 256, 0, st>>>(a); break;
+            default: k_kpoint_plain<T, 8><<<g, 256, 0, st>>>(a); break;
+        }
     } else {
-        QG_TRY(launch_stencil_tma<T>(a, 8, st, 2));
+        QG_TRY(launch_stencil_tma<T>(a, h->order, st, 2));
     }
     if (pt) pt->mark(2, st);
     if (nonlocal) {
@@ -513,7 +565,7 @@ int apply_z_checked(qg_hamiltonian h, int ns, const T* X, long long ldx, T* HX, 
     if (ns == 0) return QG_OK;
     const long long N = h->N();
     if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     T* coef = nullptr;
     if (h->pj.na > 0) {
@@ -531,7 +583,7 @@ int apply_zk_checked(qg_hamiltonian h, int nk, const double* kvecs, int nsk, con
     const long long N = h->N();
     if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
     if (nk > 1 && (ldk < (long long)nsk * ldx || ldkh < (long long)nsk * ldhx)) return QG_ERR_INVALID;
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     T* coef = nullptr;
     if (h->pj.na > 0) {
@@ -568,7 +620,7 @@ int qg_hamiltonian_apply_timed_z(qg_hamiltonian h, int ns, const double* X, long
     if (!h || ns <= 0 || !X || !HX || !ms_phases) return QG_ERR_INVALID;
     const long long N = h->N();
     if (ldx < 2 * N || ldhx < 2 * N) return QG_ERR_INVALID;
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     double* coef = nullptr;
     if (h->pj.na > 0) {

@@ -709,7 +709,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
                qg_lobpcg_report* rep) {
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
     if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
-    if (comps == 2 && h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (comps == 2 && h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3 && opt->precision != QG_FP32)
         return QG_ERR_UNSUPPORTED;
     if (opt->precond < 0 || opt->precond > 2) return QG_ERR_INVALID;
@@ -1007,7 +1007,7 @@ constexpr double kJacobiResidual = 1e-3;
 int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const double* kv, int nb, double* ev,
                   double* X_dev, double* P_dev, qg_lobpcg_report* rep) {
     if (!h || !opt || nk <= 0 || nb <= 0 || !kv || !ev || !X_dev) return QG_ERR_INVALID;
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     if (opt->precision != QG_FP64) return QG_ERR_UNSUPPORTED;
     if (opt->precond < 0 || opt->precond > 1) return QG_ERR_INVALID;
     const long long N = h->N();

@@ -178,6 +178,24 @@ constexpr int kHostChunks = 8;
 int host_pipelined_apply(qg_hamiltonian h, int ns, long long row, const double* X, double* HX,
                          const std::function<int(int, const double*, double*)>& apply);
 
+// Opts a kernel in to the device's largest dynamic shared memory (the opt-in maximum
+// less the kernel's static shared memory). Every launcher sets this same value, so
+// host threads that launch one kernel with different shared-memory sizes at once (the
+// concurrent cell solves) never lower the limit under each other's launches.
+template <typename K>
+inline cudaError_t allow_max_dynamic_smem(K* kern) {
+    int dev = 0, mx = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kern));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(reinterpret_cast<const void*>(kern), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                mx - (int)fa.sharedSizeBytes);
+}
+
 // Launch with `cluster_x` blocks per thread-block cluster along x (1: no cluster).
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_clustered(void (*kern)(KArgs...), dim3 grid, dim3 block, int cluster_x, size_t smem,

@@ -432,7 +432,7 @@ int qg_td_taylor4_z(qg_hamiltonian h, int ns, double dt, double* X, long long ld
     if (ns == 0) return QG_OK;
     const long long N = h->N();
     if (ldx < 2 * N) return QG_ERR_INVALID;
-    if (h->order != 8) return QG_ERR_UNSUPPORTED;
+    if (h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     cudaStream_t st = h->ctx->stream;
     const long long ldw = 2 * N;

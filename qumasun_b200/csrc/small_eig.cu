@@ -612,7 +612,7 @@ int small_heg_launch(const double2* A, const double2* B, int lda, long long stri
     if (k <= 0 || k > kSmallHegMax || batch <= 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = small_heg_smem(k);
     if (smem > 48 * 1024)
-        QG_CUDA_TRY(cudaFuncSetAttribute(k_small_heg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        QG_CUDA_TRY(allow_max_dynamic_smem(k_small_heg));
     k_small_heg<<<batch, kThreads, smem, st>>>(A, B, lda, stride_ab, k, skip, Z, ldz, stride_z, w, stride_w, info,
                                                pivot_floor);
     QG_CUDA_TRY(cudaGetLastError());
@@ -630,7 +630,7 @@ int small_eig_launch(const double* A, const double* B, int lda, long long stride
     if (k <= 0 || k > kSmallEigMax || batch <= 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = small_eig_smem(k);
     if (smem > 48 * 1024) {
-        QG_CUDA_TRY(cudaFuncSetAttribute(k_small_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        QG_CUDA_TRY(allow_max_dynamic_smem(k_small_eig));
     }
     k_small_eig<<<batch, kThreads, smem, st>>>(A, B, lda, stride_ab, k, n_restart, Z, ldz, stride_z, w, stride_w,
                                                info);

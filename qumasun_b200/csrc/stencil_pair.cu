@@ -324,7 +324,7 @@ int launch_pair_order(const HamArgs<T>& a, cudaStream_t st) {
     if (nst < 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = kBarBytes + (size_t)nst * stage;
     auto kern = k_stencil_pair<T, ORDER, NXC>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (allow_max_dynamic_smem(kern) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * a.ty;
     const int threads = 32 + ncons;

@@ -121,16 +121,42 @@ __device__ __forceinline__ T lap_point(T c, const T* xm, const T* xp, const T* y
     }
 }
 
-// g.grad of one point with the 8th-order first derivative (672, -168, 32, -3)/840h,
-// grouped as in LaplasianKpoint8th_halo_f (GridDifferenceKpoint8th.h:18-122); the
-// factor 2*coef and g are folded into a.dx/dy/dz.
-template <typename T>
+// g.grad of one point with the first derivative of the FD order: 8th (672, -168, 32, -3)/840h,
+// 6th (45, -9, 1)/60h, 2nd 1/2h, grouped as in LaplasianKpoint{8th,6th,2nd}_halo_f
+// (GridDifferenceKpoint8th.h:18-122, 6th.h:19-107, 2nd.h:19-92); the factor 2*coef and g
+// are folded into a.dx/dy/dz.
+template <typename T, int ORDER>
 __device__ __forceinline__ T der_point(const T* xm, const T* xp, const T* ym, const T* yp, const T* zm,
                                        const T* zp, const HamArgs<T>& a) {
-    T g = a.dx[3] * (xp[3] - xm[3]) + a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
-    g += a.dy[3] * (yp[3] - ym[3]) + a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
-    g += a.dz[3] * (zp[3] - zm[3]) + a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
-    return g;
+    if constexpr (ORDER == 2) {
+        T g = a.dx[0] * (xp[0] - xm[0]);
+        g += a.dy[0] * (yp[0] - ym[0]);
+        g += a.dz[0] * (zp[0] - zm[0]);
+        return g;
+    } else if constexpr (ORDER == 6) {
+        T g = a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
+        g += a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
+        g += a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
+        return g;
+    } else {
+        T g = a.dx[3] * (xp[3] - xm[3]) + a.dx[2] * (xp[2] - xm[2]) + a.dx[1] * (xp[1] - xm[1]) + a.dx[0] * (xp[0] - xm[0]);
+        g += a.dy[3] * (yp[3] - ym[3]) + a.dy[2] * (yp[2] - ym[2]) + a.dy[1] * (yp[1] - ym[1]) + a.dy[0] * (yp[0] - ym[0]);
+        g += a.dz[3] * (zp[3] - zm[3]) + a.dz[2] * (zp[2] - zm[2]) + a.dz[1] * (zp[1] - zm[1]) + a.dz[0] * (zp[0] - zm[0]);
+        return g;
+    }
+}
+
+// -1/2 (Lap - g^2) of one point for complex k-point states: orders 6 and 8 as lap_point
+// (a.c0 carrying -coef g^2); order 2 grouped as LaplasianKpoint2nd_halo_f
+// (GridDifferenceKpoint2nd.h:69-72), c0 p + cx (p+x + p-x) + cy (..) + cz (..).
+template <typename T, int ORDER>
+__device__ __forceinline__ T lap_point_k(T c, const T* xm, const T* xp, const T* ym, const T* yp, const T* zm,
+                                         const T* zp, const HamArgs<T>& a) {
+    if constexpr (ORDER == 2) {
+        return a.c0 * c + a.cx[0] * (xp[0] + xm[0]) + a.cy[0] * (yp[0] + ym[0]) + a.cz[0] * (zp[0] + zm[0]);
+    } else {
+        return lap_point<T, ORDER>(c, xm, xp, ym, yp, zm, zp, a);
+    }
 }
 
 constexpr int kBarBytes = 1024;  // mbarriers + control words at the front of dynamic shared memory
@@ -364,8 +390,12 @@ __global__ void __launch_bounds__(NC == 1 ? kMaxThreads : kMaxThreadsKp, 1)
                             zm[d - 1] = q[cc][sl(k, R - d)].e[e];
                             zp[d - 1] = q[cc][sl(k, R + d)].e[e];
                         }
-                        lap[cc][e] = lap_point<T, ORDER>(q[cc][sl(k, R)].e[e], xm, xp, ym, yp, zm, zp, ak);
-                        if constexpr (NC == 2) der[cc][e] = der_point<T>(xm, xp, ym, yp, zm, zp, ak);
+                        if constexpr (NC == 2) {
+                            lap[cc][e] = lap_point_k<T, ORDER>(q[cc][sl(k, R)].e[e], xm, xp, ym, yp, zm, zp, ak);
+                            der[cc][e] = der_point<T, ORDER>(xm, xp, ym, yp, zm, zp, ak);
+                        } else {
+                            lap[cc][e] = lap_point<T, ORDER>(q[cc][sl(k, R)].e[e], xm, xp, ym, yp, zm, zp, ak);
+                        }
                     }
                 }
                 __syncwarp(wmask);
@@ -481,7 +511,7 @@ int launch_order(const HamArgs<T>& a, cudaStream_t st) {
     if (nst < 0) return QG_ERR_UNSUPPORTED;
     const size_t smem = kBarBytes + (size_t)nst * stage;
     auto kern = k_stencil_tma<T, ORDER, PX, NC, NXC>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (allow_max_dynamic_smem(kern) != cudaSuccess)
         return QG_ERR_UNSUPPORTED;
     const int ncons = (a.nx / PX) * a.ty;
     const int threads = 32 + ncons;
@@ -511,7 +541,7 @@ bool stencil_tma_ok(const HamArgs<T>& a, int order, int nc) {
     constexpr int PX = 16 / sizeof(T);
     const int R = order == 2 ? 1 : (order == 8 ? 4 : 3);
     if (nc != 1 && nc != 2) return false;
-    if (nc == 2 && (order != 8 || (a.xim % PX) || (a.hxim % PX))) return false;
+    if (nc == 2 && ((order != 2 && order != 6 && order != 8) || (a.xim % PX) || (a.hxim % PX))) return false;
     if (a.row) return false;  // the nonlocal scatter runs in k_scatter_all on this path
     if (a.nx % PX != 0 || ((uintptr_t)a.X % 16) || ((uintptr_t)a.HX % 16) || ((uintptr_t)a.V % 16) ||
         (a.ldx % PX) || (a.ldhx % PX) || !a.err || a.ny < 2 * R || a.nx < 2 * R)
@@ -529,7 +559,13 @@ int launch_stencil_tma(const HamArgs<T>& a, int order, cudaStream_t st, int nc) 
     if (!stencil_tma_ok<T>(a, order, nc)) return QG_ERR_UNSUPPORTED;
     HamArgs<T> b = a;
     b.ty = tma_tile_rows(a, nc, order);
-    if (nc == 2) return launch_order<T, 8, 2>(b, st);
+    if (nc == 2) {
+        switch (order) {
+            case 2: return launch_order<T, 2, 2>(b, st);
+            case 6: return launch_order<T, 6, 2>(b, st);
+            default: return launch_order<T, 8, 2>(b, st);
+        }
+    }
     switch (order) {
         case 2: return launch_order<T, 2, 1>(b, st);
         case 4: return launch_order<T, 4, 1>(b, st);

@@ -109,6 +109,11 @@ def make_kpoint():
         out[f"{name}_g"] = np.array(gs)
         for i, g in enumerate(gs):
             out[f"{name}_HX{i}"] = O.hamiltonian_kpoint_apply(cell, g, X, impl="ref")
+            # FD orders 2 and 6 (LaplasianKpoint2nd / 6th) at the general k-vector too
+            if i == 2:
+                for order in (2, 6):
+                    out[f"{name}_HX{i}_o{order}"] = O.hamiltonian_kpoint_apply(cell, g, X, impl="ref",
+                                                                            fd_order=order)
     np.savez_compressed(os.path.join(HERE, "ham_kpoint.npz"), **out)
     print("wrote ham_kpoint")
 

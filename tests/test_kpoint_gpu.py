@@ -53,6 +53,25 @@ def test_kpoint_matches_reference_golden(cuda_ctx, gold, name, plain):
         assert rel_per_state(HX - loc, ref - loc).max() < 1e-10, (name, i)
 
 
+@pytest.mark.parametrize("plain", [False, True], ids=["tma", "plain"])
+@pytest.mark.parametrize("order", [2, 6])
+@pytest.mark.parametrize("name", sorted(KPOINT_CASES))
+def test_kpoint_fd_orders_2_6_match_reference_golden(cuda_ctx, gold, name, order, plain):
+    """FD orders 2 and 6 of the k-point operator (LaplasianKpoint2nd / 6th of the
+    reference, KINETIC_2ND / KINETIC_6TH in qumasun_kpoint.matrix.h) at the general
+    k-vector, both stencil kernels."""
+    import torch
+    from qumasun_b200 import Hamiltonian
+    cell = build_cell(**KPOINT_CASES[name])
+    X = gold[f"{name}_X"]
+    g = gold[f"{name}_g"][2]
+    H = Hamiltonian(cuda_ctx, cell, fd_order=order, kvec=tuple(g))
+    H.set_stencil_kernel(plain)
+    HX = H.apply_z(torch.from_numpy(np.ascontiguousarray(X)).cuda()).cpu().numpy()
+    H.close()
+    assert rel_per_state(HX, gold[f"{name}_HX2_o{order}"]).max() < TOL64
+
+
 def test_kpoint_diamond8_general_k_and_kvector_switch(cuda_ctx):
     import torch
     from qumasun_b200 import Hamiltonian
