@@ -9,8 +9,8 @@
 //   T  = [x_new | p_new]  (rotation outputs)
 // One iteration:
 //   Ar = H r                                       (qg::apply_hamiltonian / _z)
-//   Sa = W^T AW dV, Sb = W^T W dV                  (DSYRKX / DSYRK, lower triangles; DGEMM for
-//                                                   complex; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
+//   Sa = W^T AW dV, Sb = W^T W dV                  (lower-triangle blocks of a K-split batched DGEMM;
+//                                                   DGEMM for complex; w_dgemm path, lobpcg_d_multi_mpi.h:191-250)
 //   Sa z = lambda Sb z, k = 3n (2n on the first step of a first call), Jacobi-equilibrated,
 //   cusolverDnDsygvd / Zhegvd (replaces DSYGVX / ZHEGVX, w_dsygvx.h:24-104, UPLO as the
 //   reference); if B is not positive definite the step is solved on B's nonsingular subspace
@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "gram_mixed.h"
+#include "gram_split.h"
 #include "gram_ts.h"
 #include "precond.h"
 #include "qg_internal.h"
@@ -376,6 +377,7 @@ struct Solver {
     DevBuf W, AW, T, S, E, small, work, heg;  // heg: batched complex pencils (k-point solve)
     DevBuf gts;                                // partial sums of the tall-skinny Gram kernel
     DevBuf upd;                                // steady-state Gram reuse: blocks, products, factors
+    qg::SplitTn sp_full, sp_upd;               // K-split batched Gram products (full pencil, r blocks)
     double *UA = nullptr, *UB = nullptr, *Tu = nullptr, *fx_d = nullptr, *fp_d = nullptr;
     bool have_update = false;                  // UA/UB hold the rotated x/p blocks of the last step
     int lwork = 0;
@@ -393,6 +395,7 @@ struct Solver {
     ~Solver() {
         W.release(); AW.release(); T.release(); S.release(); E.release(); small.release();
         work.release(); heg.release(); gts.release(); upd.release();
+        sp_full.release(); sp_upd.release();
     }
 
     int setup() {
@@ -458,8 +461,8 @@ struct Solver {
     // a tall product, W^T Ar dV and W^T r dV over W = [x r p] (2 * 2 N 3n n flops against
     // 2 N (3n)^2 for the full lower triangles); the x/p blocks come from prepare_update.
     int gram_update(int k3) {
-        QG_TRY(gemm_tn(k3, n, x, Ar, dV, Sa + (size_t)n * k3, k3));
-        QG_TRY(gemm_tn(k3, n, x, r, dV, Sb + (size_t)n * k3, k3));
+        const std::vector<qg::TnBlock> blocks{{x, Ar, Sa + (size_t)n * k3}, {x, r, Sb + (size_t)n * k3}};
+        QG_TRY(sp_upd.run(blas, st, N, N, k3, n, blocks, k3, dV));
         k_place_blocks<<<n, 128, 0, st>>>(Sa, k3, n, UA, fx_d, fp_d);
         k_place_blocks<<<n, 128, 0, st>>>(Sb, k3, n, UB, fx_d, fp_d);
         QG_CUDA_TRY(cudaGetLastError());
@@ -527,8 +530,10 @@ struct Solver {
     }
 
     // Sa = W^T AW dV, Sb = W^T W dV over the leading m real columns. For real
-    // states both are symmetric and only their lower triangles are formed
-    // (DSYRKX / DSYRK, half the flops; the eigensolvers read the lower triangle);
+    // states both are symmetric and only their lower triangles are formed, as n x n
+    // blocks of one K-split batched DGEMM (qg::SplitTn; DSYRKX / DSYRK, which cost as
+    // much as the full squares at these shapes, only for m not a multiple of n; the
+    // eigensolvers read the lower triangle);
     // the split-complex Gram is not symmetric column by column, so it takes full DGEMMs.
     int gram(int m) {
         if (mixed) {
@@ -547,6 +552,18 @@ struct Solver {
         if (c == 2) {
             QG_TRY(gemm_tn(m, m, x, Ax, dV, Sa, m));
             return gemm_tn(m, m, x, x, dV, Sb, m);
+        }
+        if (m % n == 0) {
+            // lower triangles in n x n blocks, K split over one batched DGEMM
+            const int q = m / n;
+            std::vector<qg::TnBlock> blocks;
+            for (int j = 0; j < q; ++j)
+                for (int i = j; i < q; ++i) {
+                    const size_t off = (size_t)i * n + (size_t)j * n * m;
+                    blocks.push_back({x + (size_t)i * n * N, Ax + (size_t)j * n * N, Sa + off});
+                    blocks.push_back({x + (size_t)i * n * N, x + (size_t)j * n * N, Sb + off});
+                }
+            return sp_full.run(blas, st, N, N, n, n, blocks, m, dV);
         }
         const double beta = 0.0;
         QG_BLAS_TRY(cublasDsyrkx(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, m, (int)N, &dV, x, (int)N, Ax, (int)N,
