@@ -522,7 +522,8 @@ def lobpcg_diamond216(ctx):
     216-atom 3x3x3 cell (120^3, atoms displaced by seeded Gaussian sigma 0.05 bohr),
     kinetic-preconditioned GPU LOBPCG from the same seeded uniform(-0.5, 0.5) states:
     FP64 Gram products against split-BF16x3 (QG_MIXED_BF16X3) and FP32 (QG_FP32) Gram
-    products, which must agree on the 480 eigenvalues to 1e-8 Ha."""
+    products, which must agree on the 480 eigenvalues to 1e-8 Ha, and the FP64 solve once
+    more with the projection sums split over 2-block clusters (iteration-count sensitivity)."""
     import numpy as np
     import torch
     from qumasun_b200 import Hamiltonian
@@ -534,7 +535,10 @@ def lobpcg_diamond216(ctx):
     X0 = torch.rand(ns, cell.N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
     runs = {}
     evs = {}
-    for name, prec in (("fp64", 0), ("bf16x3_gram", 2), ("fp32_gram", 1)):
+    # fp64_proj2: the FP64 solve again with every atom's projection summed over a 2-block
+    # cluster (a change in the last bits of H), the sensitivity check of the iteration
+    for name, prec in (("fp64", 0), ("bf16x3_gram", 2), ("fp32_gram", 1), ("fp64_proj2", 0)):
+        H.set_nonlocal_blocking(project_parts=2 if name == "fp64_proj2" else 0)
         X = X0.clone()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -553,9 +557,11 @@ def lobpcg_diamond216(ctx):
     H.close()
     diff = float(np.abs(evs["fp64"] - evs["bf16x3_gram"]).max())
     diff32 = float(np.abs(evs["fp64"] - evs["fp32_gram"]).max())
+    diffp2 = float(np.abs(evs["fp64"] - evs["fp64_proj2"]).max())
     return {"workload": "diamond216_120cube_480of528states_fd8_kinetic_precond", **runs,
             "max_abs_ev_diff_mixed_vs_fp64_Ha": diff,
             "max_abs_ev_diff_fp32_gram_vs_fp64_Ha": diff32,
+            "max_abs_ev_diff_proj2_vs_fp64_Ha": diffp2,
             "speedup_mixed_vs_fp64": round(runs["fp64"]["seconds"] / runs["bf16x3_gram"]["seconds"], 3),
             "speedup_fp32_gram_vs_fp64": round(runs["fp64"]["seconds"] / runs["fp32_gram"]["seconds"], 3)}
 
@@ -772,6 +778,19 @@ def run_gpu_arm(a):
                    "state_applications_per_s": round(r["states_per_s"], 3)}
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+        if sweep and cpu and cpu.get("value") is not None:
+            # the reference CPU H-apply at every FD order of the sweep (FP64: the reference's
+            # H path is double only), same processes and sample as the order-8 baseline
+            for order in (2, 4, 6, 8):
+                try:
+                    r = (cpu_reference_rate(states_per_proc=1, order=order) if order != FD_ORDER
+                         else {"states_per_s": cpu["state_applications_per_s"]})
+                    sw = sweep[f"o{order}_f64"]
+                    sw["reference_cpu_state_apps_per_s"] = round(r["states_per_s"], 2)
+                    sw["reference_cpu_GBs"] = round(r["states_per_s"] * nbytes / NS / 1e9, 3)
+                    sw["speedup_vs_reference_cpu"] = round(sw["state_apps_per_s"] / r["states_per_s"], 1)
+                except Exception as ex:
+                    sweep[f"o{order}_f64"]["reference_cpu_state_apps_per_s"] = f"failed: {ex}"
 
     scf = None
     if solo and not a.no_scf:

@@ -129,6 +129,8 @@ def ref_lib():
         lib.ref_ylm_cube.argtypes = [C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp]
         lib.ref_hamiltonian_kpoint_apply.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double,
                                                      C.c_double, C.c_double, C.c_int, _dp, _dp]
+        lib.ref_lobpcg_d_mpi.argtypes = [C.POINTER(HamDescC), C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int,
+                                         _dp, _dp, _ip]
         lib.ref_lobpcg_z_multi.argtypes = [C.POINTER(HamDescC), C.c_double, C.c_double, C.c_double,
                                            C.c_double, C.c_int, C.c_int, _dp, _dp, C.c_int, _ip]
         lib.ref_potential_lda.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp] * 7
@@ -243,6 +245,30 @@ def ref_lobpcg_d_multi(cell, X0, iter_max, P0=None, first=True, quiet=True):
                                  _ptr(P, _dp), 1 if first else 0, 1 if quiet else 0,
                                  C.byref(iters))
     return dict(ev=ev, X=X, P=P, iters=iters.value, seconds=time.perf_counter() - t0)
+
+
+def ref_lobpcg_d_mpi(cell, X0, iter_max, threads=8, quiet=True, in_place=False):
+    """The reference's distributed real solver LOBPCG::Eigen_d_multi_mpi
+    (lobpcg_d_multi_mpi.h:882-1572) on one rank, SCF step 0, DGEMMs on `threads`
+    OpenBLAS threads. X0 (ns, N) is left unchanged unless in_place (then it must be a
+    C-contiguous float64 array and receives the states; no copy is made). Returns the
+    eigenvalues, states, iterations, the phase seconds (H applications, Gram, rotation,
+    n x n GEMMs, small eigensolve, rest, total) of the reference's own watch sections
+    and the seconds of each iteration."""
+    X = X0 if in_place else _c64(X0).copy()
+    if in_place and (X.dtype != np.float64 or not X.flags.c_contiguous):
+        raise ValueError("in_place needs a C-contiguous float64 array")
+    ns = X.shape[0]
+    ev = np.zeros(ns)
+    ph = np.zeros(7)
+    its = np.zeros(max(1, iter_max))
+    iters = C.c_int(0)
+    desc = HamDesc(cell)
+    ref_lib().ref_lobpcg_d_mpi(C.byref(desc.c), ns, iter_max, threads, _ptr(ev, _dp), _ptr(X, _dp),
+                               1 if quiet else 0, _ptr(ph, _dp), _ptr(its, _dp), C.byref(iters))
+    names = ("hamiltonian", "gram", "rotation", "small_gemm", "eigensolve", "rest", "total")
+    return dict(ev=ev, X=X, iters=iters.value, phase_s={k: float(v) for k, v in zip(names, ph)},
+                iteration_s=[float(v) for v in its[:iter_max]])
 
 
 def ref_lobpcg_z_multi(cell, g, X0, iter_max, quiet=True):

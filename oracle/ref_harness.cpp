@@ -65,6 +65,7 @@ inline int lapack_DSYGVX(double* A, double* B, double* ev, double* evec, double*
 #include "lobpcg_d_multi.h"
 #include "debug_print.h"
 #include "lobpcg_z_multi_mpi.h"
+#include "lobpcg_d_multi_mpi.h"
 
 /* PseudoPotIntegrator_single keeps its per-atom tables private; the harness
  * fills them directly instead of going through the .vps radial loader. */
@@ -90,6 +91,32 @@ namespace {
 struct NullWatch {
     void Record(int) {}
     void Record(int, int) {}
+};
+
+double wall_now() {
+    timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+/* The reference's watch protocol: Record(id) closes a section that began at the
+ * previous Record. Each section's time goes to its id, less the H applications
+ * (OpeA) that ran inside it, which are counted apart. */
+struct PhaseWatch {
+    double last = wall_now();
+    double acc[32] = {};
+    double h_total = 0.0, h_since = 0.0;
+    void Record(int id) {
+        const double t = wall_now();
+        if (id >= 0 && id < 32) acc[id] += (t - last) - h_since;
+        last = t;
+        h_since = 0.0;
+    }
+    void Record(int id, int) { Record(id); }
+    void add_h(double dt) {
+        h_total += dt;
+        h_since += dt;
+    }
 };
 
 struct QuietStdout {
@@ -517,6 +544,67 @@ int ref_hamiltonian_kpoint_apply(const ref_ham_desc* d, double gx, double gy, do
 }  // extern "C"
 
 extern "C" {
+
+/* The reference's distributed real LOBPCG (LOBPCG::Eigen_d_multi_mpi,
+ * lobpcg_d_multi_mpi.h:882-1572) on one rank with the reference H as OpeA (one state
+ * per call, no OPERATION_BUNDLE), SCF_step 0 (P starts from zero), no kept S matrix,
+ * DGEMMs on `threads` OpenBLAS threads, iter_max iterations. X (ns*N) in/out, ev (ns)
+ * out. phase_s[7] receives seconds: [0] H (every OpeA call), [1] Gram (the GEMM1
+ * section, watch id 17, without its H calls), [2] rotation (GEMM2, id 16), [3] n x n
+ * GEMMs (GEMM3, id 19), [4] small eigensolve (LAPACK, id 15), [5] the rest (ids 10, 14),
+ * [6] the whole call; iter_s[iter_max] (may be null) the seconds of each iteration, from
+ * its first H application to the next one's. *iters receives the iterations taken
+ * (from OpeA calls). */
+int ref_lobpcg_d_mpi(const ref_ham_desc* d, int ns, int iter_max, int threads, double* ev, double* X, int quiet,
+                     double* phase_s, double* iter_s, int* iters) {
+    RefHamiltonian H(d);
+    const size_t N = (size_t)d->nx * d->ny * d->nz;
+    const double dV = d->hx * d->hy * d->hz;
+    GridRangeMPI grid;
+    std::memset(static_cast<void*>(&grid), 0, sizeof(grid));
+    grid.end_x = d->nx; grid.end_y = d->ny; grid.end_z = d->nz;
+    grid.mpi_comm = MPI_COMM_WORLD;
+    if (threads > 0) scipy_openblas_set_num_threads(threads);
+    std::vector<double> keep((size_t)ns * N, 0.0);
+    std::vector<double> work((size_t)5 * ns * N, 0.0);
+    long long calls = 0;
+    PhaseWatch watch;
+    std::vector<double> batch_start;  // wall time of the first OpeA call of every ns-state batch
+    auto OpeA = [&](double* Ax, double* x) {
+        ++calls;
+        const double t0 = wall_now();
+        if ((calls - 1) % ns == 0) batch_start.push_back(t0);
+        H.Apply(Ax, x);
+        watch.add_h(wall_now() - t0);
+    };
+    const double t0 = wall_now();
+    {
+        QuietStdout q(quiet != 0);
+        LOBPCG::Eigen_d_multi_mpi(grid, dV, ns, iter_max, ev, X, keep.data(), work.data(), (double*)nullptr, 0,
+                                  OpeA, watch);
+    }
+    const double t_end = wall_now();
+    if (iter_s) {
+        // batches 0 and 1 are the initial A x and A p; iteration i starts with batch 2 + i
+        for (int i = 0; i < iter_max; ++i) {
+            const size_t b = 2 + (size_t)i;
+            iter_s[i] = b < batch_start.size()
+                            ? (b + 1 < batch_start.size() ? batch_start[b + 1] : t_end) - batch_start[b]
+                            : 0.0;
+        }
+    }
+    if (phase_s) {
+        phase_s[0] = watch.h_total;
+        phase_s[1] = watch.acc[17];
+        phase_s[2] = watch.acc[16];
+        phase_s[3] = watch.acc[19];
+        phase_s[4] = watch.acc[15];
+        phase_s[5] = watch.acc[10] + watch.acc[14];
+        phase_s[6] = t_end - t0;
+    }
+    if (iters) *iters = (int)((calls - 2LL * ns) / ns);
+    return 0;
+}
 
 /* The reference's complex block LOBPCG (Eigen_z_multi_mpi) on one rank with the
  * reference k-point Hamiltonian as OpeA, SCF_step 0 (P starts from zero), run

@@ -7,7 +7,10 @@
 //
 // Persistent kernel, one CTA per SM, 10 warps:
 //   warp 0      TMA producer: 128 x 64 bf16 tiles of every piece of A and B
-//               (cp.async.bulk.tensor.2d, 128-byte swizzle) into a ring of S stages;
+//               (cp.async.bulk.tensor.2d, 128-byte swizzle) into a ring of S stages; the
+//               pieces are stored K-block-major ([N / 64][m][64]), so each tile is one
+//               contiguous 16 KB run (column-major pieces spread a tile over 128 columns
+//               N * 2 bytes apart, which at N = 1.7 M halved the kernel's rate);
 //   warp 1      owns 256 TMEM columns (two 128 x 128 FP32 accumulators); one lane
 //               issues tcgen05.mma.cta_group::1.kind::f16 (M = N = 128, K = 16) for
 //               every product and K step of a stage, then tcgen05.commit frees the
@@ -240,8 +243,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     mbar_expect_tx(&full[j], kStageBytes);
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
-                        tma_load_2d(st + p * kTileBytes, &tm.a[p], kb * BK, ti * BM, &full[j]);
-                        tma_load_2d(st + (P + p) * kTileBytes, &tm.b[p], kb * BK, tj * BM, &full[j]);
+                        // pieces are K-block-major: block kb holds the 64-row segments of all
+                        // m columns, so a 128-column tile is one contiguous 16 KB run
+                        tma_load_2d(st + p * kTileBytes, &tm.a[p], 0, kb * u.m + ti * BM, &full[j]);
+                        tma_load_2d(st + (P + p) * kTileBytes, &tm.b[p], 0, kb * u.m + tj * BM, &full[j]);
                     }
                     ctl[1] = pos;
                 }
@@ -349,29 +354,40 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // C(i, j) = alpha * sum_seg part[seg][tile(i, j)][i % 128][j % 128], C column-major (ld ldc);
-// lower: only i >= j (the tiles of the lower triangle).
+// lower: only the tiles of the lower triangle (ti >= tj). Threads walk the partial tiles
+// contiguously (the segments' reads are coalesced); the segments add in order.
 __global__ void k_gram_reduce(const double* __restrict__ part, Units u, double alpha, double* __restrict__ C,
                               int ldc) {
-    const long long total = (long long)u.m * u.m;
+    const long long total = (long long)u.ntiles * (BM * BM);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const int j = (int)(e / u.m), i = (int)(e - (long long)j * u.m);
-        const int ti = i / BM, tj = j / BM;
-        if (u.lower && ti < tj) continue;
-        const int t = u.lower ? ti * (ti + 1) / 2 + tj : ti * u.tiles_m + tj;
-        const size_t off = (size_t)(i % BM) * BM + (j % BM);
+        const int t = (int)(e / (BM * BM));
+        const int off = (int)(e - (long long)t * (BM * BM));
+        int seg, ti, tj;
+        unit_coords(t, u, seg, ti, tj);
+        const int i = ti * BM + off / BM, j = tj * BM + off % BM;
+        if (i >= u.m || j >= u.m) continue;
         double s = 0.0;
         for (int sg = 0; sg < u.nseg; ++sg) s += part[((size_t)sg * u.ntiles + t) * (BM * BM) + off];
         C[i + (long long)j * ldc] = alpha * s;
     }
 }
 
+// The P bf16 pieces of the N x m block src (column-major, ld N), K-block-major:
+// dst[p][((k / 64) * m + j) * 64 + k % 64] for row k and column j, rows N .. kpad-1 of the
+// last block zero (kpad = N rounded up to 64).
 template <int P>
-__global__ void k_split_pieces(const double* __restrict__ src, long long n, __nv_bfloat16* __restrict__ dst,
-                               long long piece_stride) {
+__global__ void k_split_pieces(const double* __restrict__ src, long long N, int m, long long kpad,
+                               __nv_bfloat16* __restrict__ dst, long long piece_stride) {
+    const long long n = kpad * m;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        double v = src[i];
+        const long long blk = i >> 6;  // (k / 64) * m + j
+        const int r = (int)(i & 63);
+        const long long kb = blk / m;
+        const int j = (int)(blk - kb * m);
+        const long long k = kb * BK + r;
+        double v = k < N ? src[(long long)j * N + k] : 0.0;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             const __nv_bfloat16 h = __double2bfloat16(v);
@@ -398,11 +414,13 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap* map, const __nv_bfloat16* ptr, long long N, int m) {
+// Tensor map of one K-block-major piece: a 2-D array of 64-element (128-byte) rows,
+// kblocks * m of them; a box is 128 consecutive rows (one tile, K-major).
+int make_map(CUtensorMap* map, const __nv_bfloat16* ptr, long long kblocks, int m) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return QG_ERR_UNSUPPORTED;
-    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)m};
-    const cuuint64_t strides[1] = {(cuuint64_t)N * 2};
+    const cuuint64_t dims[2] = {(cuuint64_t)BK, (cuuint64_t)(kblocks * m)};
+    const cuuint64_t strides[1] = {(cuuint64_t)BK * 2};
     const cuuint32_t box[2] = {BK, BM};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult rc = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims, strides,
@@ -426,26 +444,28 @@ int sm_count_dev() {
 
 }  // namespace
 
-bool TcGram::supported(long long N) { return N % 8 == 0 && N >= BK && encode_fn() != nullptr; }
+bool TcGram::supported(long long N) { return N >= BK && encode_fn() != nullptr; }
+
+long long TcGram::kpad() const { return (N + BK - 1) / BK * BK; }
 
 int TcGram::setup(long long N_, int mmax_, int pieces_) {
     if (pieces_ != 2 && pieces_ != 3) return QG_ERR_INVALID;
     N = N_;
     mmax = mmax_;
     pieces = pieces_;
-    QG_TRY(split_a.reserve((size_t)pieces * N * mmax * sizeof(__nv_bfloat16)));
+    QG_TRY(split_a.reserve((size_t)pieces * kpad() * mmax * sizeof(__nv_bfloat16)));
     return QG_OK;  // the B-side slot is allocated by the first split into it
 }
 
 int TcGram::split(const double* A, int m, int which, cudaStream_t st) {
     DevBuf& b = which == 0 ? split_a : split_b;
-    QG_TRY(b.reserve((size_t)pieces * N * mmax * sizeof(__nv_bfloat16)));
-    const long long n = N * m;
-    const long long ps = N * mmax;
+    if (m <= 0 || m > mmax) return QG_ERR_INVALID;
+    QG_TRY(b.reserve((size_t)pieces * kpad() * mmax * sizeof(__nv_bfloat16)));
+    const long long ps = kpad() * mmax;
     if (pieces == 2)
-        k_split_pieces<2><<<148 * 8, 256, 0, st>>>(A, n, b.as<__nv_bfloat16>(), ps);
+        k_split_pieces<2><<<148 * 8, 256, 0, st>>>(A, N, m, kpad(), b.as<__nv_bfloat16>(), ps);
     else
-        k_split_pieces<3><<<148 * 8, 256, 0, st>>>(A, n, b.as<__nv_bfloat16>(), ps);
+        k_split_pieces<3><<<148 * 8, 256, 0, st>>>(A, N, m, kpad(), b.as<__nv_bfloat16>(), ps);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
 }
@@ -455,10 +475,11 @@ int TcGram::gram(cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, 
     std::memset(&tm, 0, sizeof(tm));
     const __nv_bfloat16* A = split_a.as<__nv_bfloat16>();
     const __nv_bfloat16* B = b_is_a ? A : split_b.as<__nv_bfloat16>();
-    const long long ps = N * mmax;
+    if (m <= 0 || m > mmax) return QG_ERR_INVALID;
+    const long long ps = kpad() * mmax;
     for (int p = 0; p < pieces; ++p) {
-        QG_TRY(make_map(&tm.a[p], A + p * ps, N, m));
-        QG_TRY(make_map(&tm.b[p], B + p * ps, N, m));
+        QG_TRY(make_map(&tm.a[p], A + p * ps, kpad() / BK, m));
+        QG_TRY(make_map(&tm.b[p], B + p * ps, kpad() / BK, m));
     }
     Units u;
     u.m = m;

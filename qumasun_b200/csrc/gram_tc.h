@@ -9,11 +9,13 @@ struct TcGram {
     int mmax = 0, pieces = 3;
     DevBuf split_a, split_b, part;
 
-    // N a multiple of 8 (16-byte row pitch of the bf16 pieces) and the driver's
-    // tensor-map encoder available
+    // N >= 64 and the driver's tensor-map encoder available
     static bool supported(long long N);
+    // N rounded up to the 64-row K block (rows of the pieces, zero past N)
+    long long kpad() const;
     int setup(long long N, int mmax, int pieces);
-    // bf16 pieces of the N x m block A (ld N) into slot `which` (0: A side, 1: B side)
+    // bf16 pieces of the N x m block A (ld N, m <= mmax) into slot `which` (0: A side,
+    // 1: B side), stored K-block-major; gram() must be given the same m
     int split(const double* A, int m, int which, cudaStream_t st);
     // C (m x m, column-major, ld ldc) = alpha * A^T B from the split slots (B = A when
     // b_is_a); lower: only the tiles on and below the diagonal are computed and
