@@ -15,11 +15,12 @@
 //               issues tcgen05.mma.cta_group::1.kind::f16 (M = N = 128, K = 16) for
 //               every product and K step of a stage, then tcgen05.commit frees the
 //               stage and hands the accumulator to the epilogue;
-//   warps 2-9   epilogue: tcgen05.ld of the accumulator after EVERY 64-row K block,
-//               added into FP64 registers (each thread: one tile row, 64 columns),
-//               so the FP32 accumulation spans one K block only (the tensor cores'
-//               FP32 sums drift on long same-sign runs); the accumulator buffers
-//               alternate so the MMAs of block k+1 overlap the read-out of block k.
+//   warps 2-9   epilogue: tcgen05.ld of the accumulator after every 64-row K block
+//               (3 pieces; every second block for 2 pieces), added into FP64 registers
+//               (each thread: one tile row, 64 columns), so the FP32 accumulation spans
+//               64 (128) rows only (the tensor cores' FP32 sums drift on long same-sign
+//               runs); the accumulator buffers alternate so the MMAs of the next block
+//               overlap the read-out of the last.
 // Work units are (tile, K segment), K-segment-major so that concurrent CTAs stream
 // the same rows of A and B (L2 reuse); every unit writes its FP64 partial tile once,
 // and k_gram_reduce sums the segments in a fixed order (deterministic).
@@ -43,6 +44,12 @@ constexpr int kThreads = 320;
 constexpr int kTileBytes = BM * BK * 2;  // 16 KB per piece tile
 constexpr int kEpiWarps = 8;
 constexpr int kAccCols = 128;
+// 64-row K blocks summed in FP32 (TMEM) between read-outs: 2 for the 2-piece split
+// (47.6 against 56.4 ms at N = 1.728 M x 1584, error unchanged at its 2^-18 level), 1 for
+// the 3-piece split (the same 79 ms either way, while 2 doubles its FP32 drift on
+// norm-like entries to 1.4e-6)
+template <int P>
+constexpr int readout_blocks() { return P == 2 ? 2 : 1; }
 
 struct TMaps {
     CUtensorMap a[3];
@@ -260,11 +267,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                 int seg, ti, tj;
                 unit_coords(unit, u, seg, ti, tj);
                 const int kb0 = seg * u.kb_per_seg, kb1 = min(u.kblocks, kb0 + u.kb_per_seg);
-                for (int kb = kb0; kb < kb1; ++kb, ++pos, ++accpos) {
+                for (int kb = kb0; kb < kb1; ++kb, ++pos) {
                     const int j = pos % S, k = pos / S;
                     const int buf = accpos & 1, n = accpos >> 1;
+                    constexpr int RO = readout_blocks<P>();
+                    const bool first = (kb - kb0) % RO == 0;
+                    const bool last = (kb - kb0) % RO == RO - 1 || kb == kb1 - 1;
                     bool ok = mbar_wait(&full[j], (uint32_t)k & 1u);
-                    if (ok && n > 0) ok = mbar_wait(&accempty[buf], (uint32_t)(n - 1) & 1u);
+                    if (ok && first && n > 0) ok = mbar_wait(&accempty[buf], (uint32_t)(n - 1) & 1u);
                     if (!ok || ctl[0]) {
                         ctl[0] = 1;
                         if (!ok) atomicExch(err, (int)QG_ERR_TIMEOUT);
@@ -279,11 +289,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                         for (int q = 0; q < Products<P>::n; ++q) {
                             const uint64_t ad = sw128_desc(st + Products<P>::a(q) * kTileBytes) + 2 * kk;
                             const uint64_t bd = sw128_desc(st + (P + Products<P>::b(q)) * kTileBytes) + 2 * kk;
-                            umma_f16(d, ad, bd, (kk | q) ? 1u : 0u);
+                            umma_f16(d, ad, bd, (!first || kk || q) ? 1u : 0u);
                         }
                     }
-                    umma_commit(&empty[j]);     // the stage is free once these MMAs have read it
-                    umma_commit(&accfull[buf]); // the accumulator holds this K block
+                    umma_commit(&empty[j]);  // the stage is free once these MMAs have read it
+                    if (last) {
+                        umma_commit(&accfull[buf]);  // the accumulator holds this group of K blocks
+                        ++accpos;
+                    }
                 }
             }
             umma_commit(done);  // completes once every MMA issued above has finished
@@ -304,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int seg, ti, tj;
             unit_coords(unit, u, seg, ti, tj);
             const int kb0 = seg * u.kb_per_seg, kb1 = min(u.kblocks, kb0 + u.kb_per_seg);
-            for (int kb = kb0; kb < kb1; ++kb, ++accpos) {
+            for (int kb = kb0; kb < kb1; kb += readout_blocks<P>(), ++accpos) {
                 const int buf = accpos & 1, n = accpos >> 1;
                 const bool ok = mbar_wait(&accfull[buf], (uint32_t)n & 1u);
                 if (__any_sync(0xffffffffu, !ok || ctl[0] != 0)) {
