@@ -211,7 +211,10 @@ typedef struct qg_lobpcg_options {
     int verbose;        /* 1: print (iteration, max residual) lines to stdout */
     int precond;        /* 0: none (the reference's solvers); 1: kinetic, w = (-1/2 Lap_FD + shift)^-1 r
                            applied in Fourier space with the FD stencil's own symbol; 2: kinetic
-                           plus the learned correction of qg_hamiltonian_set_learned */
+                           plus the learned correction of qg_hamiltonian_set_learned; 3: kinetic,
+                           with the learned correction NN(r) as a fourth block of the
+                           Rayleigh-Ritz basis [x, T r, NN(r), p] (real states, QG_FP64; one more
+                           H application per iteration) */
     double precond_shift; /* shift (Ha) of the kinetic preconditioner; <= 0 selects 1.0 */
     int n_converge;     /* the lowest n_converge states must meet tol, the others are a guard
                            band against a degenerate multiplet at the cut; <= 0 or >= ns: all */

@@ -380,6 +380,8 @@ struct Solver {
     qg::SplitTn sp_full, sp_upd;               // K-split batched Gram products (full pencil, r blocks)
     double *UA = nullptr, *UB = nullptr, *Tu = nullptr, *fx_d = nullptr, *fp_d = nullptr;
     bool have_update = false;                  // UA/UB hold the rotated x/p blocks of the last step
+    int nblk = 3;                              // blocks of W: [x r p], or [x r q p] with the learned block q
+    double *q = nullptr, *Aq = nullptr;        // the learned block (nblk = 4)
     int lwork = 0;
     double *x, *r, *p, *Ax, *Ar, *Ap, *Tx, *Tp, *Sa, *Sb, *Sa2, *Sb2, *M;
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
@@ -400,10 +402,10 @@ struct Solver {
 
     int setup() {
         const size_t blk = (size_t)L * n;
-        QG_TRY(W.reserve(3 * blk * sizeof(double)));
-        QG_TRY(AW.reserve(3 * blk * sizeof(double)));
+        QG_TRY(W.reserve(nblk * blk * sizeof(double)));
+        QG_TRY(AW.reserve(nblk * blk * sizeof(double)));
         QG_TRY(T.reserve(2 * blk * sizeof(double)));
-        const size_t k3 = 3 * (size_t)n, g3 = c * k3;
+        const size_t k3 = (size_t)nblk * n, g3 = c * k3;  // the largest pencil
         // real Gram pair (c k3)^2 each; the equilibrated pencil (k3^2 real or complex each);
         // for c = 2 the real rotation matrix (2 k3 x 2 n)
         QG_TRY(S.reserve((2 * g3 * g3 + 2 * c * k3 * k3 + (c == 2 ? g3 * 2 * n : 0)) * sizeof(double)));
@@ -411,8 +413,12 @@ struct Solver {
         QG_TRY(E.reserve(4 * (size_t)c * k3 * k3 * sizeof(double)));
         E0 = E.as<double>();
         s_h.resize(k3);
-        x = W.as<double>(); r = x + blk; p = r + blk;
-        Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + blk;
+        x = W.as<double>(); r = x + blk; p = r + (nblk - 2) * blk;
+        Ax = AW.as<double>(); Ar = Ax + blk; Ap = Ar + (nblk - 2) * blk;
+        if (nblk == 4) {
+            q = r + blk;
+            Aq = Ar + blk;
+        }
         Tx = T.as<double>(); Tp = Tx + blk;
         Sa = S.as<double>(); Sb = Sa + g3 * g3; Sa2 = Sb + g3 * g3; Sb2 = Sa2 + c * k3 * k3;
         M = Sb2 + c * k3 * k3;
@@ -729,12 +735,16 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     if (comps == 2 && h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
     if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3 && opt->precision != QG_FP32)
         return QG_ERR_UNSUPPORTED;
-    if (opt->precond < 0 || opt->precond > 2) return QG_ERR_INVALID;
-    if (opt->precond == 2 && !h->learned) return QG_ERR_INVALID;
+    if (opt->precond < 0 || opt->precond > 3) return QG_ERR_INVALID;
+    if (opt->precond >= 2 && !h->learned) return QG_ERR_INVALID;
+    // precond 3 (the learned block): real states and FP64 Gram products only
+    const bool aug = opt->precond == 3;
+    if (aug && (comps != 1 || opt->precision != QG_FP64)) return QG_ERR_UNSUPPORTED;
     const long long N = h->N();
-    if ((long long)n * 3 > N) return QG_ERR_INVALID;
+    if ((long long)n * (aug ? 4 : 3) > N) return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(h->ctx->device));
     Solver s;
+    s.nblk = aug ? 4 : 3;
     s.h = h;
     s.n = n;
     s.c = comps;
@@ -792,13 +802,21 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     }
     qg::KineticPrecond* pc = nullptr;
     const bool learned = opt->precond == 2;
-    // w = T r (precond 1), w = T r + NN(r) (precond 2: the learned correction, learned.cu)
+    // w = T r (precond 1), w = T r + NN(r) (precond 2: the learned correction, learned.cu);
+    // precond 3: w = T r and the network's correction as a block of its own, q = NN(r),
+    // so the Rayleigh-Ritz step chooses how much of it to take (its basis [x, T r, q, p]
+    // contains the kinetic method's [x, T r, p])
     auto precondition = [&]() -> int {
-        if (learned) QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.r, blk_bytes, cudaMemcpyDeviceToDevice, st));
+        if (learned || aug) QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.r, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_TRY(pc->apply(s.r, st));
         if (learned)
             QG_TRY(qg_learned_apply_d(h->learned, h->nx, h->ny, h->nz, comps * n, s.Tx, N, h->V_d, h->learned_vscale,
                                       s.r, N, 1));
+        if (aug) {
+            QG_TRY(qg_learned_apply_d(h->learned, h->nx, h->ny, h->nz, n, s.Tx, N, h->V_d, h->learned_vscale, s.q, N,
+                                      0));
+            s.normalize(s.q, nullptr);
+        }
         s.normalize(s.r, nullptr);
         return QG_OK;
     };
@@ -829,14 +847,16 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
+        if (aug) QG_TRY(s.applyH(s.q, s.Aq));
         tm.mark(1, st);
         const bool two = (first && it == 0) || restart_2n;
         restart_2n = false;
-        const int k3 = (two ? 2 : 3) * n;
+        // pencil columns: [x r (q) p], without p on a 2n step
+        const int k3 = ((two ? 2 : 3) + (aug ? 1 : 0)) * n;
         // steady state: the x/p blocks of the pencil come from the last rotation and only
         // the r blocks are tall products; a full Gram every kFullGramEvery iterations, after
         // a 2n step, a rank-revealing solve or a rollback, and in the reduced-precision phase
-        const bool use_update = s.have_update && !two && !s.mixed && (it % kFullGramEvery) != 0;
+        const bool use_update = s.have_update && !two && !s.mixed && !aug && (it % kFullGramEvery) != 0;
         if (use_update) QG_TRY(s.gram_update(k3));
         else QG_TRY(s.gram(c * k3));
         s.have_update = false;
@@ -869,7 +889,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         // and the A-side blocks are re-applied, Ax = H x_new, Ap = H p_new, instead of
         // rotated: two memory-bound H applications cost less than the two tall DGEMMs
         // and keep Ax consistent with x for the residual.
-        const bool next_update = h->gram_reuse && c == 1 && !s.mixed && !restarted && 3 * n > qg::kGramTsUpTo;
+        const bool next_update =
+            h->gram_reuse && c == 1 && !s.mixed && !aug && !restarted && 3 * n > qg::kGramTsUpTo;
         if (next_update) QG_TRY(s.prepare_update(Z, ldz, k3));
         QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp, 0.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
