@@ -537,7 +537,8 @@ def lobpcg_diamond216(ctx):
     evs = {}
     # fp64_proj2: the FP64 solve again with every atom's projection summed over a 2-block
     # cluster (a change in the last bits of H), the sensitivity check of the iteration
-    for name, prec in (("fp64", 0), ("bf16x3_gram", 2), ("fp32_gram", 1), ("fp64_proj2", 0)):
+    for name, prec in (("fp64", 0), ("bf16x3_gram", 2), ("fp32_gram", 1), ("fp64_proj2", 0),
+                       ("fp64_int8_gram", 3)):
         H.set_nonlocal_blocking(project_parts=2 if name == "fp64_proj2" else 0)
         X = X0.clone()
         torch.cuda.synchronize()
@@ -558,10 +559,13 @@ def lobpcg_diamond216(ctx):
     diff = float(np.abs(evs["fp64"] - evs["bf16x3_gram"]).max())
     diff32 = float(np.abs(evs["fp64"] - evs["fp32_gram"]).max())
     diffp2 = float(np.abs(evs["fp64"] - evs["fp64_proj2"]).max())
+    diffi8 = float(np.abs(evs["fp64"] - evs["fp64_int8_gram"]).max())
     return {"workload": "diamond216_120cube_480of528states_fd8_kinetic_precond", **runs,
             "max_abs_ev_diff_mixed_vs_fp64_Ha": diff,
             "max_abs_ev_diff_fp32_gram_vs_fp64_Ha": diff32,
             "max_abs_ev_diff_proj2_vs_fp64_Ha": diffp2,
+            "max_abs_ev_diff_int8_gram_vs_fp64_Ha": diffi8,
+            "speedup_int8_gram_vs_fp64": round(runs["fp64"]["seconds"] / runs["fp64_int8_gram"]["seconds"], 3),
             "speedup_mixed_vs_fp64": round(runs["fp64"]["seconds"] / runs["bf16x3_gram"]["seconds"], 3),
             "speedup_fp32_gram_vs_fp64": round(runs["fp64"]["seconds"] / runs["fp32_gram"]["seconds"], 3)}
 
@@ -873,7 +877,7 @@ def gram_leg(ctx, N=1_728_000, m=1584, steps=5):
     Cm = torch.zeros(m, m, dtype=torch.float64, device="cuda")
     ref = A @ A.T
     out = {"N": N, "m": m}
-    for pieces in (3, 2, 0):
+    for pieces in (3, 2, 0, 7):
         rc = lib().qg_gram_mixed_d(ctx.h, N, m, C.c_void_p(A.data_ptr()), None, 1.0, C.c_void_p(Cm.data_ptr()), pieces)
         if rc != 0:
             out[f"pieces{pieces}"] = {"status": rc}

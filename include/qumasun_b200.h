@@ -43,8 +43,13 @@ typedef enum qg_status {
  * 8 use cuBLAS BF16 GEMMs on 2 pieces) until the residual falls below 1e-6 or stops
  * halving, then as FP64; H, residuals, rotations, norms and the small eigensolves
  * stay FP64 throughout (a solve that reaches the tolerance or max_iter while still
- * mixed takes an FP64 Rayleigh-Ritz on X before its residuals are judged). */
-typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2 } qg_precision;
+ * mixed takes an FP64 Rayleigh-Ritz on X before its residuals are judged).
+ * QG_FP64_INT8 (LOBPCG, real states): an FP64 iteration whose Gram products (pencils of
+ * more than 128 columns) run on the tensor cores' int8 path: each column scaled by a
+ * power of two and cut into 7 exact 7-bit slices, the 28 slice products with exact int32
+ * accumulation, the scale groups added in FP64 -- as accurate as DGEMM (no counterpart in
+ * the reference, whose Gram products are BLAS DGEMMs). */
+typedef enum qg_precision { QG_FP64 = 0, QG_FP32 = 1, QG_MIXED_BF16X3 = 2, QG_FP64_INT8 = 3 } qg_precision;
 
 typedef struct qg_context_s* qg_context;
 typedef struct qg_hamiltonian_s* qg_hamiltonian;
@@ -305,8 +310,9 @@ int qg_lobpcg_cells_device(int ncells, const qg_hamiltonian* hams, const qg_lobp
  * pieces = 2 or 3 bf16 pieces per value on the library's tcgen05 kernel (FP32
  * accumulation over one 64-row K block, FP64 across blocks; N a multiple of 8),
  * pieces = 0 the cuBLAS BF16 hi/lo path (FP32 over 1024-row chunks), pieces = -1
- * FP32 copies and FP32 GEMMs over the same chunks (the Gram of QG_FP32). Waits for
- * the stream; returns QG_ERR_UNSUPPORTED if the tcgen05 path cannot take N. */
+ * FP32 copies and FP32 GEMMs over the same chunks (the Gram of QG_FP32), pieces = 7
+ * the FP64-accurate int8 slice products of QG_FP64_INT8. Waits for the stream; returns
+ * QG_ERR_UNSUPPORTED if the tensor-core path cannot take N. */
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha,
                     double* C, int pieces);
 

@@ -59,6 +59,8 @@ int MixedGram::setup(long long N_, int mmax_, int pieces_) {
     N = N_;
     mmax = mmax_;
     pieces = pieces_;
+    use_i8 = pieces == kI8Slices && I8Gram::supported(N);
+    if (pieces == kI8Slices) return use_i8 ? i8.setup(N, mmax) : QG_ERR_UNSUPPORTED;
     use_tc = pieces > 0 && TcGram::supported(N);
     if (use_tc) return tc.setup(N, mmax, pieces);
     const size_t elems = (size_t)N * mmax;
@@ -73,6 +75,7 @@ int MixedGram::setup(long long N_, int mmax_, int pieces_) {
 }
 
 int MixedGram::split(const double* A, int m, int which, cudaStream_t st) {
+    if (use_i8) return i8.split(A, m, which, st);
     if (use_tc) return tc.split(A, m, which, st);
     const long long n = N * m;
     DevBuf& b = which == 0 ? split_a : split_b;
@@ -90,6 +93,7 @@ int MixedGram::split(const double* A, int m, int which, cudaStream_t st) {
 
 int MixedGram::gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, double* C,
                     int ldc, int* err) {
+    if (use_i8) return i8.gram(st, m, b_is_a, lower, alpha, C, ldc, err);
     if (use_tc) return tc.gram(st, m, b_is_a, lower, alpha, C, ldc, err);
     if (pieces < 0) return gram_fp32(blas, st, m, b_is_a, alpha, C, ldc);
     const __nv_bfloat16* ahi = split_a.as<__nv_bfloat16>();
@@ -169,6 +173,7 @@ int MixedGram::gram_fp32(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_
 
 void MixedGram::release() {
     tc.release();
+    i8.release();
     split_a.release();
     split_b.release();
     part.release();
@@ -187,7 +192,9 @@ extern "C" {
 
 int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const double* B, double alpha, double* C,
                     int pieces) {
-    if (!ctx || N <= 0 || m <= 0 || !A || !C || pieces < -1 || pieces > 3 || pieces == 1) return QG_ERR_INVALID;
+    if (!ctx || N <= 0 || m <= 0 || !A || !C || pieces < -1 || (pieces > 3 && pieces != qg::kI8Slices) ||
+        pieces == 1)
+        return QG_ERR_INVALID;
     QG_CUDA_TRY(cudaSetDevice(ctx->device));
     cublasHandle_t blas;
     QG_TRY(qg_blas_handle(ctx, &blas));
@@ -199,7 +206,7 @@ int qg_gram_mixed_d(qg_context ctx, long long N, int m, const double* A, const d
         ctx->gram_cache = g;
         QG_TRY(g->setup(N, m, pieces));
     }
-    if (pieces > 0 && !g->use_tc) return QG_ERR_UNSUPPORTED;
+    if (pieces > 0 && !g->use_tc && !g->use_i8) return QG_ERR_UNSUPPORTED;
     QG_TRY(g->split(A, m, 0, ctx->stream));
     const bool same = (B == nullptr || B == A);
     if (!same) QG_TRY(g->split(B, m, 1, ctx->stream));

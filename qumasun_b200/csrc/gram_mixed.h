@@ -2,6 +2,7 @@
 #pragma once
 #include <cublas_v2.h>
 
+#include "gram_i8.h"
 #include "gram_tc.h"
 #include "qg_internal.h"
 
@@ -23,6 +24,9 @@ struct MixedGram {
     int pieces = 3;
     bool use_tc = false;
     TcGram tc;
+    // pieces = kI8Slices (7): FP64-accurate products on the int8 tensor cores (gram_i8.cu)
+    bool use_i8 = false;
+    I8Gram i8;
 
     int setup(long long N, int mmax, int pieces = 3);
     // bf16 pieces of the N x m block A (ld N) into slot `which` (0: A side, 1: B side)
@@ -32,6 +36,13 @@ struct MixedGram {
     int gram(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, bool lower, double alpha, double* C,
              int ldc, int* err);
     int gram_fp32(cublasHandle_t blas, cudaStream_t st, int m, bool b_is_a, double alpha, double* C, int ldc);
+    // C (ma x nc, ld ldc) = alpha * A^T B with A = slot 0's first ma columns and B = columns
+    // b_off .. of slot b_slot: the int8 path only (QG_ERR_UNSUPPORTED otherwise)
+    int gram_rect(cudaStream_t st, int ma, int nc, int b_slot, int b_off, double alpha, double* C, int ldc,
+                  int* err) {
+        if (!use_i8) return QG_ERR_UNSUPPORTED;
+        return i8.gram_rect(st, ma, nc, b_slot, b_off, alpha, C, ldc, err);
+    }
     void release();
     ~MixedGram() { release(); }
 };

@@ -387,6 +387,7 @@ struct Solver {
     double* E0;  // rank-revealing solve scratch: basis, product, reduced pencil, vectors (k3 x k3 each)
     std::vector<double> s_h;
     bool mixed = false;      // reduced-precision Gram products (qg::MixedGram) until the hand-over
+    bool i8 = false;         // FP64-accurate Gram products on the int8 tensor cores (QG_FP64_INT8)
     int mixed_pieces = 3;    // qg::MixedGram split: 3 = split-BF16x3 on tcgen05, -1 = FP32
     double trunc_eps = 1e-12;  // relative eigenvalue floor of B in the rank-revealing solve
     qg::MixedGram mg;
@@ -450,6 +451,7 @@ struct Solver {
         QG_TRY(h->coef.reserve((c == 1 ? qg::coef_scratch_elems(h, n) : qg::coef_scratch_elems_z(h, 1, n)) *
                                sizeof(double)));
         if (mixed) QG_TRY(mg.setup(N, (int)g3, mixed_pieces));
+        if (i8 && c == 1) QG_TRY(mg.setup(N, (int)g3, qg::kI8Slices));
         if (c == 1) {
             const size_t nn = (size_t)n * n;
             QG_TRY(upd.reserve((6 * nn + 2 * k3 * (size_t)n + 2 * (size_t)n) * sizeof(double)));
@@ -467,8 +469,16 @@ struct Solver {
     // a tall product, W^T Ar dV and W^T r dV over W = [x r p] (2 * 2 N 3n n flops against
     // 2 N (3n)^2 for the full lower triangles); the x/p blocks come from prepare_update.
     int gram_update(int k3) {
-        const std::vector<qg::TnBlock> blocks{{x, Ar, Sa + (size_t)n * k3}, {x, r, Sb + (size_t)n * k3}};
-        QG_TRY(sp_upd.run(blas, st, N, N, k3, n, blocks, k3, dV));
+        if (i8) {
+            // [x r p]^T Ar and [x r p]^T r (the A side's own columns n .. 2n-1) on the int8 path
+            QG_TRY(mg.split(x, k3, 0, st));
+            QG_TRY(mg.split(Ar, n, 1, st));
+            QG_TRY(mg.gram_rect(st, k3, n, 1, 0, dV, Sa + (size_t)n * k3, k3, h->ctx->dev_status));
+            QG_TRY(mg.gram_rect(st, k3, n, 0, n, dV, Sb + (size_t)n * k3, k3, h->ctx->dev_status));
+        } else {
+            const std::vector<qg::TnBlock> blocks{{x, Ar, Sa + (size_t)n * k3}, {x, r, Sb + (size_t)n * k3}};
+            QG_TRY(sp_upd.run(blas, st, N, N, k3, n, blocks, k3, dV));
+        }
         k_place_blocks<<<n, 128, 0, st>>>(Sa, k3, n, UA, fx_d, fp_d);
         k_place_blocks<<<n, 128, 0, st>>>(Sb, k3, n, UB, fx_d, fp_d);
         QG_CUDA_TRY(cudaGetLastError());
@@ -558,6 +568,13 @@ struct Solver {
         if (c == 2) {
             QG_TRY(gemm_tn(m, m, x, Ax, dV, Sa, m));
             return gemm_tn(m, m, x, x, dV, Sb, m);
+        }
+        if (i8) {
+            // lower triangles from the int8 Ozaki products (gram_i8.cu): as accurate as DGEMM
+            QG_TRY(mg.split(x, m, 0, st));
+            QG_TRY(mg.split(Ax, m, 1, st));
+            QG_TRY(mg.gram(blas, st, m, false, true, dV, Sa, m, h->ctx->dev_status));
+            return mg.gram(blas, st, m, true, true, dV, Sb, m, h->ctx->dev_status);
         }
         if (m % n == 0) {
             // lower triangles in n x n blocks, K split over one batched DGEMM
@@ -733,7 +750,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     if (!h || !opt || n <= 0 || !ev) return QG_ERR_INVALID;
     if (comps == 1 && (h->gx != 0.0 || h->gy != 0.0 || h->gz != 0.0)) return QG_ERR_INVALID;
     if (comps == 2 && h->order != 2 && h->order != 6 && h->order != 8) return QG_ERR_UNSUPPORTED;
-    if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3 && opt->precision != QG_FP32)
+    if (opt->precision != QG_FP64 && opt->precision != QG_MIXED_BF16X3 && opt->precision != QG_FP32 &&
+        opt->precision != QG_FP64_INT8)
         return QG_ERR_UNSUPPORTED;
     if (opt->precond < 0 || opt->precond > 3) return QG_ERR_INVALID;
     if (opt->precond >= 2 && !h->learned) return QG_ERR_INVALID;
@@ -753,6 +771,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     s.dV = h->hx * h->hy * h->hz;
     s.st = h->ctx->stream;
     s.mixed = opt->precision == QG_MIXED_BF16X3 || opt->precision == QG_FP32;
+    s.i8 = opt->precision == QG_FP64_INT8 && comps == 1 && qg::I8Gram::supported(N);
     s.mixed_pieces = opt->precision == QG_FP32 ? -1 : 3;
     s.trunc_eps = s.mixed ? 1e-6 : 1e-12;
     QG_TRY(qg_blas_handle(h->ctx, &s.blas));

@@ -6,14 +6,15 @@ unrelated columns (A^T B) 5e-8 with 3 pieces; norm-like entries (A^T A, same-sig
 sums) carry the tensor cores' FP32 accumulation drift, ~7 ulp of the K block's
 partial sum, so 2e-6 with 3 pieces; 2 pieces (a_lo b_lo dropped, ~2^-18 on
 norm-like entries) and the cuBLAS path 1e-5; pieces = -1 (FP32 copies, FP32 GEMMs over
-1024-row chunks, the Gram of QG_FP32) 1e-6."""
+1024-row chunks, the Gram of QG_FP32) 1e-6; pieces = 7 (the int8 slice products of
+QG_FP64_INT8, exact int32 sums) 1e-13, DGEMM's level."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-BOUND = {3: (5e-8, 2e-6), 2: (1e-5, 1e-5), 0: (1e-5, 1e-5), -1: (1e-6, 1e-6)}
+BOUND = {3: (5e-8, 2e-6), 2: (1e-5, 1e-5), 0: (1e-5, 1e-5), -1: (1e-6, 1e-6), 7: (1e-13, 1e-13)}
 
 
 def run_gram(ctx, A, B, pieces):
@@ -28,7 +29,7 @@ def run_gram(ctx, A, B, pieces):
     return C64
 
 
-@pytest.mark.parametrize("pieces", [3, 2, 0, -1])
+@pytest.mark.parametrize("pieces", [3, 2, 0, -1, 7])
 @pytest.mark.parametrize("N,m", [(64_000, 300), (200_000, 96), (1_728_000, 64)])
 def test_gram_mixed_matches_fp64(cuda_ctx, N, m, pieces):
     import torch
