@@ -742,6 +742,9 @@ constexpr int kFullGramEvery = 10;
 // Largest |1 - |x'_j|^2 dV| of a rotated Ritz vector before the step is rolled back, and
 // the rollbacks a solve may take before it stops (QG_ERR_CHOLESKY).
 constexpr double kNormDrift = 1.0e-3;
+// A step whose largest residual grew by more than this factor over the last step's is
+// taken as a breakdown of the reused Gram blocks: the next Gram is a full one.
+constexpr double kResidualJump = 100.0;
 constexpr int kMaxRollbacks = 20;
 
 int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps, double* ev, double* X_dev,
@@ -863,21 +866,26 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
     double best_res = 1e300;
     int best_it = 0, mixed_iters = s.mixed ? opt->max_iter : 0;
     bool restart_2n = false;  // after a norm-drift rollback: the next step uses the [x r] pencil
+    bool used_update = false;  // this step's pencil came from the reused Gram blocks
+    double last_res = 1e300;
     for (it = 0; it < opt->max_iter; ++it) {
         tm.mark(0, st);
         QG_TRY(s.applyH(s.r, s.Ar));
         if (aug) QG_TRY(s.applyH(s.q, s.Aq));
         tm.mark(1, st);
         const bool two = (first && it == 0) || restart_2n;
+        const bool after_rollback = restart_2n;
         restart_2n = false;
         // pencil columns: [x r (q) p], without p on a 2n step
         const int k3 = ((two ? 2 : 3) + (aug ? 1 : 0)) * n;
         // steady state: the x/p blocks of the pencil come from the last rotation and only
-        // the r blocks are tall products; a full Gram every kFullGramEvery iterations, after
-        // a 2n step, a rank-revealing solve or a rollback, and in the reduced-precision phase
+        // the r blocks are tall products; a full Gram every kFullGramEvery iterations, on a 2n
+        // step, after a rank-revealing solve, on both steps after a rollback, after a step
+        // whose residual jumped by kResidualJump, and in the reduced-precision phase
         const bool use_update = s.have_update && !two && !s.mixed && !aug && (it % kFullGramEvery) != 0;
         if (use_update) QG_TRY(s.gram_update(k3));
         else QG_TRY(s.gram(c * k3));
+        used_update = use_update;
         s.have_update = false;
         tm.mark(2, st);
         // Jacobi-equilibrated pencil (keeps the tiny residual columns of the reference
@@ -909,7 +917,7 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
         // rotated: two memory-bound H applications cost less than the two tall DGEMMs
         // and keep Ax consistent with x for the residual.
         const bool next_update =
-            h->gram_reuse && c == 1 && !s.mixed && !aug && !restarted && 3 * n > qg::kGramTsUpTo;
+            h->gram_reuse && c == 1 && !s.mixed && !aug && !restarted && !after_rollback && 3 * n > qg::kGramTsUpTo;
         if (next_update) QG_TRY(s.prepare_update(Z, ldz, k3));
         QG_TRY(s.gemm_nn(c * (k3 - n), c * n, s.r, Z + c * n, ldz, s.Tp, 0.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
@@ -969,6 +977,8 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             ++it;
             break;
         }
+        if (s.have_update && used_update && maxres > kResidualJump * last_res) s.have_update = false;
+        last_res = maxres;
         if (opt->verbose) printf("lobpcg iter %d max residual %.3e%s\n", it + 1, maxres, s.mixed ? " (bf16x3)" : "");
         if (s.mixed && maxres < tol * s.dV) {
             // the mixed iteration reached the tolerance: FP64 Rayleigh-Ritz on X and an
