@@ -867,7 +867,8 @@ def run_gpu_arm(a):
 def gram_leg(ctx, N=1_728_000, m=1584, steps=5):
     """Split-BF16 Gram products of the mixed-precision LOBPCG at the 216-atom cell's
     shape (N = 120^3 rows, m = 3 x 528 columns): the tcgen05 kernel with 3 and 2
-    pieces and the cuBLAS BF16 path against FP64 DGEMM, time and max error."""
+    pieces, the cuBLAS BF16 path and the int8 7-slice (FP64-accurate) kernel against
+    FP64 DGEMM, time and max error."""
     import ctypes as C
     import torch
     from qumasun_b200.engine import lib
