@@ -456,11 +456,40 @@ def learned_leg(ctx, steps=1500):
     Rh, Ch, Vh = LP.residual_pairs(ctx, hc, 16, (3, 8), seed=77)
     held = LP.held_out_loss(nn, [((hc.nx, hc.ny, hc.nz), Rh, Ch, Vh)])
     cmp = LP.compare(ctx, nn, build_cell(displacement=0.1, seed=98), 16, n_converge=14)
+    apply_ms = network_apply_times(nn)
     nn.close()
     return {"workload": "diamond8_40cube_train4cells_eval_unseen_sigma0.1", "pairs": sum(d[1].shape[0] for d in data),
             "pair_generation_s": round(t1 - t0, 2), "training_steps": steps, "training_s": round(t2 - t1, 2),
             "loss_history": [[s_, round(l_, 4)] for s_, l_ in hist], "held_out_loss": round(held, 4),
-            "lobpcg_unseen_cell": cmp}
+            "lobpcg_unseen_cell": cmp, "network_apply_80cube_64states": apply_ms}
+
+
+def network_apply_times(nn, grid=(80, 80, 80), ns=64, reps=5):
+    """One application of the trained network to 64 residuals on the 80^3 grid (15.1k
+    multiply-adds per voxel), CUDA events: the 16 -> 16 layers on the tensor cores
+    against the CUDA-core kernel."""
+    import torch
+    N = grid[0] * grid[1] * grid[2]
+    g = torch.Generator(device="cuda").manual_seed(3)
+    R = torch.rand(ns, N, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    V = torch.rand(N, dtype=torch.float64, device="cuda", generator=g) - 4.0
+    out = torch.zeros_like(R)
+    res = {}
+    for name, on in (("tensor_cores", True), ("cuda_cores", False)):
+        nn.set_tensor_cores(on)
+        for _ in range(2):
+            nn.apply(grid, R, V, 4.0, out=out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            nn.apply(grid, R, V, 4.0, out=out)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"ms": round(ms, 3), "TMAC_per_s": round(15120.0 * N * ns / (ms * 1e-3) / 1e12, 2)}
+    nn.set_tensor_cores(True)
+    return res
 
 
 def cells_leg():

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "qg_internal.h"
+#include "tc_common.cuh"
 
 namespace {
 
@@ -301,6 +302,200 @@ __global__ void k_scale_f(float* __restrict__ x, long long n, const double* __re
         x[i] *= s;
 }
 
+
+// ---------------------------------------------------------------------------
+// The 16 -> 16 channel layers on the 5th-generation tensor cores (sm_100a).
+// One CTA (4 warps) owns a column block of CX x CY voxels of one state and marches CZ
+// planes in z. The input's halo planes (CX+2 x CY+2 voxels) sit in shared memory split
+// into two 8-channel halves, each voxel's 8 channels one 16-byte row, so that operand A
+// of one tap -- 128 voxels (x fastest) x 16 input channels -- is the canonical K-major
+// layout without swizzle at a shifted start address: each run of 8 voxels along x is one
+// core matrix (8 rows of 16 bytes), consecutive y rows are HXC * 16 bytes apart (SBO)
+// and the second channel half one half-plane further (LBO). The 27 taps are then 27
+// tcgen05.mma.kind::f16 (M 128, N 16, K 16, BF16 in, FP32 accumulator in TMEM) with no
+// im2col copy; the weights sit as [tap][channel half][co][8 ci] (LBO 256 B, SBO 128 B).
+// After the MMAs of plane z are committed the CTA loads halo plane z + 2 (ring of 4),
+// then reads the accumulator back with tcgen05.ld (one TMEM lane per voxel), adds the
+// bias, applies ReLU and stores BF16. Same periodic convolution as k_conv_fwd; the
+// products are summed in a different order (per tap on the tensor cores).
+using namespace qg::tc;
+
+constexpr int CX = 8, CY = 16, CZ = 8;          // voxels of a CTA's column block; z planes per CTA
+constexpr int HXC = CX + 2, HYC = CY + 2;
+constexpr int kHalfB = HXC * HYC * 16;          // one 8-channel half of a halo plane (2880 B)
+constexpr int kSlotB = 2 * kHalfB;              // one halo plane
+constexpr int kSlots = 4;
+constexpr int kWB = 27 * 512;                   // weights, bf16 [tap][half][co][8]
+// shared memory: the halo ring, the weights, the mbarrier and the TMEM address (36.9 KB;
+// a tap's operand reaches at most the end of the ring)
+constexpr int kConvTcSmem = kSlots * kSlotB + kWB + 64;
+constexpr uint32_t kIdescConv = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint64_t desc_nosw(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_conv(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdescConv), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ int wrap_any(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// out (B x 16 x N) = relu(conv(in (B x 16 x N)) + bias); W bf16 [16][16][27]. Grid:
+// x = (x block, y block, z slab), y = state. Requires nx % CX == 0.
+__global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restrict__ in,
+                                                   const __nv_bfloat16* __restrict__ W,
+                                                   const float* __restrict__ bias, __nv_bfloat16* __restrict__ out,
+                                                   Grid g, int tiles_y, int* err) {
+    extern __shared__ __align__(128) unsigned char csm[];
+    unsigned char* halo = csm;
+    unsigned char* wsm = csm + kSlots * kSlotB;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + kWB);
+    volatile uint32_t* tslot = reinterpret_cast<volatile uint32_t*>(bar + 1);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int txb = g.nx / CX;
+    int blk = blockIdx.x;
+    const int xb = blk % txb;
+    blk /= txb;
+    const int yb = blk % tiles_y;
+    const int zs = blk / tiles_y;
+    const int b = blockIdx.y;
+    const int x0 = xb * CX, y0 = yb * CY, z0 = zs * CZ, z1 = min(g.nz, z0 + CZ);
+
+    if (t == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32((const void*)tslot)),
+                     "r"(32)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // weights: element ((tap * 2 + h) * 16 + co) * 8 + j = W[co][h * 8 + j][tap]
+    __nv_bfloat16* wb = reinterpret_cast<__nv_bfloat16*>(wsm);
+    for (int i = t; i < 27 * 256; i += 128) {
+        const int j = i & 7, co = (i >> 3) & 15, h = (i >> 7) & 1, tap = i >> 8;
+        wb[i] = W[(co * 16 + h * 8 + j) * 27 + tap];
+    }
+    const __nv_bfloat16* inb = in + (long long)b * 16 * g.N;
+    const int xl0 = wrap_any(x0 - 1, g.nx), xr0 = wrap_any(x0 + CX, g.nx);
+    auto load_plane = [&](int z) {  // z in [-1, nz]: halo plane z into slot (z + 4) % 4
+        const int zz = wrap_any(z, g.nz);
+        unsigned char* dst = halo + ((z + 4) & 3) * kSlotB;
+        // one (channel, y row) per step: the 8 interior voxels as one 16-byte load (x0 and
+        // nx are multiples of 8), the two periodic edge voxels as single loads
+        for (int e = t; e < 16 * HYC; e += 128) {
+            const int yh = e % HYC, ci = e / HYC;
+            const long long row = (long long)ci * g.N + (long long)g.nx * (wrap_any(y0 + yh - 1, g.ny) + (long long)g.ny * zz);
+            const uint4 mid = *reinterpret_cast<const uint4*>(inb + row + x0);
+            __nv_bfloat16 vals[HXC];
+            vals[0] = inb[row + xl0];
+            vals[HXC - 1] = inb[row + xr0];
+            const __nv_bfloat16* mv = reinterpret_cast<const __nv_bfloat16*>(&mid);
+#pragma unroll
+            for (int i = 0; i < CX; ++i) vals[1 + i] = mv[i];
+            __nv_bfloat16* rowdst = reinterpret_cast<__nv_bfloat16*>(dst + (ci >> 3) * kHalfB + yh * HXC * 16) + (ci & 7);
+#pragma unroll
+            for (int xh = 0; xh < HXC; ++xh) rowdst[xh * 8] = vals[xh];
+        }
+    };
+    load_plane(z0 - 1);
+    load_plane(z0);
+    load_plane(z0 + 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // thread stores -> tensor core reads
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
+    float bs[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) bs[c] = bias[c];
+    const int m = warp * 32 + lane, xl = m & (CX - 1), yl = m / CX;
+    uint32_t phase = 0;
+    bool bad = false;
+    for (int z = z0; z < z1; ++z) {
+        if (t == 0) {
+#pragma unroll 1
+            for (int tap = 0; tap < 27; ++tap) {
+                const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+                const uint32_t a = hbase + (uint32_t)((((z - 1 + dz) + 4) & 3) * kSlotB + (dy * HXC + dx) * 16);
+                umma_conv(tmem, desc_nosw(a, kHalfB, HXC * 16), desc_nosw(wbase + tap * 512, 256, 128),
+                          tap ? 1u : 0u);
+            }
+            umma_commit(bar);
+        }
+        if (z + 1 < z1) load_plane(z + 2);  // for plane z + 1 (the slot of plane z - 2, not read now)
+        const bool ok = mbar_wait(bar, phase);
+        if (__syncthreads_or(!ok)) {
+            bad = true;
+            break;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), r);
+        tmem_wait_ld();
+        const int y = y0 + yl;
+        if (y < g.ny) {
+            const long long v = (x0 + xl) + (long long)g.nx * (y + (long long)g.ny * z);
+            __nv_bfloat16* ob = out + (long long)b * 16 * g.N + v;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) ob[(long long)c * g.N] = __float2bfloat16(fmaxf(__uint_as_float(r[c]) + bs[c], 0.f));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if (bad) {
+        if (t == 0) {
+            atomicExch(err, (int)QG_ERR_TIMEOUT);
+            mbar_wait(bar, phase);  // bounded: the MMAs in flight finish before TMEM is freed
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+    }
+}
+
+bool conv16_tc_ok(const Grid& g, int B) {
+    if (g.nx % CX != 0 || B > 65535) return false;
+    const long long nblk = (long long)(g.nx / CX) * ((g.ny + CY - 1) / CY) * ((g.nz + CZ - 1) / CZ);
+    return nblk <= 0x7fffffffLL;
+}
+
+int launch_conv16_tc(const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias, __nv_bfloat16* out,
+                     const Grid& g, int B, int* err, cudaStream_t st) {
+    const int tiles_y = (g.ny + CY - 1) / CY;
+    const long long nblk = (long long)(g.nx / CX) * tiles_y * ((g.nz + CZ - 1) / CZ);
+    k_conv16_tc<<<dim3((unsigned)nblk, B), 128, kConvTcSmem, st>>>(in, W, bias, out, g, tiles_y, err);
+    QG_CUDA_TRY(cudaGetLastError());
+    return QG_OK;
+}
 }  // namespace
 
 struct qg_learned_s {
@@ -308,6 +503,7 @@ struct qg_learned_s {
     DevBuf master, adam_m, adam_v, grad, wbf, wtbf;  // params FP32 / BF16, transposed BF16 weights
     DevBuf act, dact, part, small, loss_acc;         // activations, gradients, partials, scratch
     int step = 0;
+    bool tensor_cores = true;  // the 16 -> 16 forward layers on tcgen05 where the grid allows
 };
 
 namespace {
@@ -337,8 +533,14 @@ int forward(qg_learned L, const Grid& g, int B, cudaStream_t st, __nv_bfloat16**
     const float* P = L->master.as<float>();  // biases are read in FP32
     const dim3 grid(g.tx * g.ty * g.tz, B);
     k_conv_fwd<2, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a0, W + woff(0), P + woff(0) + wcount(0), a1, nullptr, g);
-    k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a1, W + woff(1), P + woff(1) + wcount(1), a2, nullptr, g);
-    k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a2, W + woff(2), P + woff(2) + wcount(2), a3, nullptr, g);
+    if (L->tensor_cores && conv16_tc_ok(g, B)) {
+        int* err = L->ctx->dev_status;
+        QG_TRY(launch_conv16_tc(a1, W + woff(1), P + woff(1) + wcount(1), a2, g, B, err, st));
+        QG_TRY(launch_conv16_tc(a2, W + woff(2), P + woff(2) + wcount(2), a3, g, B, err, st));
+    } else {
+        k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a1, W + woff(1), P + woff(1) + wcount(1), a2, nullptr, g);
+        k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a2, W + woff(2), P + woff(2) + wcount(2), a3, nullptr, g);
+    }
     k_conv_fwd<16, 1, false, __nv_bfloat16, float><<<grid, TV, 0, st>>>(a3, W + woff(3), P + woff(3) + wcount(3), p, nullptr, g);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
@@ -492,6 +694,13 @@ int qg_learned_get_params(qg_learned L, float* params, int n) {
     QG_CUDA_TRY(cudaMemcpyAsync(params, L->master.ptr, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost,
                                 L->ctx->stream));
     QG_CUDA_TRY(cudaStreamSynchronize(L->ctx->stream));
+    return QG_OK;
+}
+
+int qg_learned_set_tensor_cores(qg_learned L, int on) {
+    if (!L) return QG_ERR_INVALID;
+    QG_CUDA_TRY(cudaStreamSynchronize(L->ctx->stream));
+    L->tensor_cores = on != 0;
     return QG_OK;
 }
 

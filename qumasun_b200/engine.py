@@ -139,6 +139,7 @@ def lib():
         L.qg_learned_get_params.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
         L.qg_learned_apply_d.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp, C.c_double,
                                          vp, C.c_longlong, C.c_int]
+        L.qg_learned_set_tensor_cores.argtypes = [vp, C.c_int]
         L.qg_learned_gradient.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp, C.c_double,
                                           vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_float)]
         L.qg_learned_train_step.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_longlong, vp,
@@ -387,6 +388,11 @@ class LearnedPreconditioner:
         check(lib().qg_learned_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size),
               "qg_learned_get_params")
         return p
+
+    def set_tensor_cores(self, on: bool):
+        """Run the two 16 -> 16 forward layers on the tensor cores (the default, where
+        nx is a multiple of 8) or on the CUDA-core kernel."""
+        check(lib().qg_learned_set_tensor_cores(self.h, 1 if on else 0), "qg_learned_set_tensor_cores")
 
     def apply(self, grid, R, V, vscale, out=None, accumulate=False):
         """out (+)= NN(R) for float64 CUDA tensors R (ns, N), V (N,)."""

@@ -113,3 +113,44 @@ def test_learned_block_never_worse_than_kinetic(cuda_ctx):
     np.testing.assert_allclose(np.sort(b["ev"])[:14], np.sort(a["ev"])[:14], rtol=0, atol=1e-8)
     H.close()
     nn.close()
+
+
+def test_tensor_core_layers_match_cuda_core_layers(cuda_ctx):
+    """The two 16 -> 16 forward layers on tcgen05 (halo planes in shared memory, one MMA
+    per tap) against the CUDA-core kernel on the same network and states: the same
+    output up to the order of the FP32 sums and the BF16 rounding of the activations.
+    The grid has several column blocks in x and y, a partial y block (40 = 2 x 16 + 8)
+    and a partial z slab (20 = 2 x 8 + 4)."""
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    rng = np.random.default_rng(11)
+    grid = (24, 40, 20)
+    N = grid[0] * grid[1] * grid[2]
+    P = rng.normal(0, 0.15, NN.n_params()).astype(np.float32)
+    R = torch.from_numpy(rng.normal(size=(5, N))).cuda()
+    V = torch.from_numpy(-4.0 * np.exp(-rng.uniform(0, 3, size=N))).cuda()
+    nn = LearnedPreconditioner(cuda_ctx)
+    nn.set_params(P)
+    tc = nn.apply(grid, R, V, 4.0).cpu().numpy()
+    nn.set_tensor_cores(False)
+    cc = nn.apply(grid, R, V, 4.0).cpu().numpy()
+    nn.set_tensor_cores(True)
+    tc2 = nn.apply(grid, R, V, 4.0).cpu().numpy()
+    nn.close()
+    assert np.isfinite(tc).all()
+    assert np.linalg.norm(tc - cc) / np.linalg.norm(cc) < 5e-3
+    np.testing.assert_array_equal(tc, tc2)  # deterministic
+    assert cuda_ctx.take_device_status() == 0
+
+
+def test_forward_without_tensor_core_grid_matches_oracle(cuda_ctx):
+    """nx not a multiple of 8: the forward pass keeps the CUDA-core kernel."""
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    grid, P, R, V, Y = small_case(seed=12, grid=(12, 10, 9), ns=2)
+    nn = LearnedPreconditioner(cuda_ctx)
+    nn.set_params(P)
+    out = nn.apply(grid, torch.from_numpy(R).cuda(), torch.from_numpy(V).cuda(), 4.0).cpu().numpy()
+    nn.close()
+    ref = NN.apply(P, grid, R, V, 4.0)
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 5e-3
