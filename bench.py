@@ -63,7 +63,7 @@ def parse():
                    help="skip the SCF-step leg (density, potential, Taylor-4 step, nonlocal forces)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-preconditioner leg (GPU training and an unseen-cell comparison)")
-    p.add_argument("--only", choices=["kpoint", "gram", "cells"], default=None,
+    p.add_argument("--only", choices=["kpoint", "gram", "cells", "netapply"], default=None,
                    help="run one leg alone and print its JSON (profiling captures)")
     p.add_argument("--kpoints", type=int, default=64, help="k-points of the k-point leg (4x4x4 grid order)")
     p.add_argument("--gram-rows", type=int, default=1_728_000, help="rows N of the --only gram leg")
@@ -462,6 +462,18 @@ def learned_leg(ctx, steps=1500):
             "pair_generation_s": round(t1 - t0, 2), "training_steps": steps, "training_s": round(t2 - t1, 2),
             "loss_history": [[s_, round(l_, 4)] for s_, l_ in hist], "held_out_loss": round(held, 4),
             "lobpcg_unseen_cell": cmp, "network_apply_80cube_64states": apply_ms}
+
+
+def netapply_leg(ctx, steps=5):
+    """The learned preconditioner's network alone (seeded random parameters, no
+    training): 64 residuals at 80^3, tensor-core against CUDA-core 16 -> 16 layers."""
+    import numpy as np
+    from qumasun_b200 import LearnedPreconditioner
+    nn = LearnedPreconditioner(ctx)
+    nn.set_params(np.random.default_rng(4).normal(0, 0.1, nn.n_params).astype(np.float32))
+    out = network_apply_times(nn, reps=max(1, steps))
+    nn.close()
+    return {"workload": "learned_network_80cube_64states", **out}
 
 
 def network_apply_times(nn, grid=(80, 80, 80), ns=64, reps=5):
@@ -941,6 +953,8 @@ def run_only(a):
         out = gram_leg(ctx, N=a.gram_rows, m=a.gram_cols, steps=a.steps)
     elif a.only == "cells":
         out = cells_leg()
+    elif a.only == "netapply":
+        out = netapply_leg(ctx, steps=a.steps)
     else:
         out = kpoint_leg(ctx, n_k=a.kpoints, steps=a.steps)
     print(json.dumps(out), flush=True)
