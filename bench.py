@@ -466,7 +466,7 @@ def learned_leg(ctx, steps=1500):
 
 def netapply_leg(ctx, steps=5):
     """The learned preconditioner's network alone (seeded random parameters, no
-    training): 64 residuals at 80^3, tensor-core against CUDA-core 16 -> 16 layers."""
+    training): 64 residuals at 80^3, tensor-core against CUDA-core layers."""
     import numpy as np
     from qumasun_b200 import LearnedPreconditioner
     nn = LearnedPreconditioner(ctx)
@@ -478,8 +478,8 @@ def netapply_leg(ctx, steps=5):
 
 def network_apply_times(nn, grid=(80, 80, 80), ns=64, reps=5):
     """One application of the trained network to 64 residuals on the 80^3 grid (15.1k
-    multiply-adds per voxel), CUDA events: the 16 -> 16 layers on the tensor cores
-    against the CUDA-core kernel."""
+    multiply-adds per voxel), CUDA events: the layers on the tensor cores against the
+    CUDA-core kernels."""
     import torch
     N = grid[0] * grid[1] * grid[2]
     g = torch.Generator(device="cuda").manual_seed(3)

@@ -338,11 +338,11 @@ int qg_learned_create(qg_context ctx, qg_learned* out);
 int qg_learned_destroy(qg_learned nn);
 int qg_learned_set_params(qg_learned nn, const float* params, int n);  /* HOST params */
 int qg_learned_get_params(qg_learned nn, float* params, int n);
-/* The two 16 -> 16 channel layers of the forward pass run on the tensor cores
- * (tcgen05.mma kind::f16, BF16 operands, FP32 accumulation in TMEM; one MMA per 3^3
- * tap over halo planes staged in shared memory) when nx is a multiple of 8 -- the
- * default; on = 0 selects the CUDA-core kernel for them (the two differ only in the
- * order of the FP32 sums). Waits for the stream. */
+/* The four layers of the forward pass run on the tensor cores (tcgen05.mma kind::f16,
+ * BF16 operands, FP32 accumulation in TMEM; one 16 x 16 channel MMA per 3^3 tap over
+ * halo planes staged in shared memory) when nx is a multiple of 8 -- the default;
+ * on = 0 selects the CUDA-core kernels (the two differ only in the order of the FP32
+ * sums). The backward pass always runs on the CUDA-core kernels. Waits for the stream. */
 int qg_learned_set_tensor_cores(qg_learned nn, int on);
 /* out[s] (+)= NN(R[s]) for ns states on an nx x ny x nz grid; R, V, out DEVICE FP64. */
 int qg_learned_apply_d(qg_learned nn, int nx, int ny, int nz, int ns, const double* R, long long ldr,

@@ -19,6 +19,10 @@
 //                  one thread per (ci, tap) holding all co, tile partials summed in a
 //                  fixed order (deterministic);
 //   k_adam         Adam on FP32 master weights, BF16 copies for the kernels.
+// Forward pass on the tensor cores (the default where nx is a multiple of 8):
+//   k_conv_tc      every layer as 27 tcgen05.mma per z plane over shared-memory halo
+//                  planes (described below); k_conv_fwd then serves the backward pass and
+//                  grids the tensor-core kernel does not take.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -304,7 +308,7 @@ __global__ void k_scale_f(float* __restrict__ x, long long n, const double* __re
 
 
 // ---------------------------------------------------------------------------
-// The 16 -> 16 channel layers on the 5th-generation tensor cores (sm_100a).
+// The network layers on the 5th-generation tensor cores (sm_100a).
 // One CTA (4 warps) owns a column block of CX x CY voxels of one state and marches CZ
 // planes in z. The input's halo planes (CX+2 x CY+2 voxels) sit in shared memory split
 // into two 8-channel halves, each voxel's 8 channels one 16-byte row, so that operand A
@@ -316,8 +320,11 @@ __global__ void k_scale_f(float* __restrict__ x, long long n, const double* __re
 // im2col copy; the weights sit as [tap][channel half][co][8 ci] (LBO 256 B, SBO 128 B).
 // After the MMAs of plane z are committed the CTA loads halo plane z + 2 (ring of 4),
 // then reads the accumulator back with tcgen05.ld (one TMEM lane per voxel), adds the
-// bias, applies ReLU and stores BF16. Same periodic convolution as k_conv_fwd; the
-// products are summed in a different order (per tap on the tensor cores).
+// bias, applies ReLU where the layer has one and stores (BF16 activations, FP32 for the
+// last layer). Layers with fewer channels use the same 16 x 16 MMA: the missing input
+// channels are zero in the halo, the missing outputs have zero weights and are not
+// stored. Same periodic convolution as k_conv_fwd; the products are summed in a
+// different order (per tap on the tensor cores).
 using namespace qg::tc;
 
 constexpr int CX = 8, CY = 16, CZ = 8;          // voxels of a CTA's column block; z planes per CTA
@@ -360,12 +367,16 @@ __device__ __forceinline__ int wrap_any(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
-// out (B x 16 x N) = relu(conv(in (B x 16 x N)) + bias); W bf16 [16][16][27]. Grid:
+// out (B x COUT x N) = act(conv(in (B x CIN x N)) + bias); W bf16 [COUT][CIN][27];
+// CIN, COUT <= 16 (the MMA is always 16 x 16 per tap: missing input channels are zero
+// in the halo, missing output channels have zero weights and are not stored). Grid:
 // x = (x block, y block, z slab), y = state. Requires nx % CX == 0.
-__global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restrict__ in,
-                                                   const __nv_bfloat16* __restrict__ W,
-                                                   const float* __restrict__ bias, __nv_bfloat16* __restrict__ out,
-                                                   Grid g, int tiles_y, int* err) {
+template <int CIN, int COUT, bool RELU, typename TO>
+__global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict__ in,
+                                                 const __nv_bfloat16* __restrict__ W,
+                                                 const float* __restrict__ bias, TO* __restrict__ out,
+                                                 Grid g, int tiles_y, int* err) {
+    static_assert(CIN >= 1 && CIN <= 16 && COUT >= 1 && COUT <= 16, "16 x 16 channel MMA");
     extern __shared__ __align__(128) unsigned char csm[];
     unsigned char* halo = csm;
     unsigned char* wsm = csm + kSlots * kSlotB;
@@ -392,20 +403,25 @@ __global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restri
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // weights: element ((tap * 2 + h) * 16 + co) * 8 + j = W[co][h * 8 + j][tap]
+    // weights: element ((tap * 2 + h) * 16 + co) * 8 + j = W[co][h * 8 + j][tap] (zero past CIN, COUT)
     __nv_bfloat16* wb = reinterpret_cast<__nv_bfloat16*>(wsm);
     for (int i = t; i < 27 * 256; i += 128) {
-        const int j = i & 7, co = (i >> 3) & 15, h = (i >> 7) & 1, tap = i >> 8;
-        wb[i] = W[(co * 16 + h * 8 + j) * 27 + tap];
+        const int j = i & 7, co = (i >> 3) & 15, h = (i >> 7) & 1, tap = i >> 8, ci = h * 8 + j;
+        wb[i] = (ci < CIN && co < COUT) ? W[(co * CIN + ci) * 27 + tap] : __float2bfloat16(0.f);
     }
-    const __nv_bfloat16* inb = in + (long long)b * 16 * g.N;
+    if constexpr (CIN < 16) {
+        // the channels the input lacks stay zero in every halo plane
+        for (int i = t; i < kSlots * kSlotB / 16; i += 128) reinterpret_cast<uint4*>(halo)[i] = make_uint4(0, 0, 0, 0);
+        __syncthreads();
+    }
+    const __nv_bfloat16* inb = in + (long long)b * CIN * g.N;
     const int xl0 = wrap_any(x0 - 1, g.nx), xr0 = wrap_any(x0 + CX, g.nx);
     auto load_plane = [&](int z) {  // z in [-1, nz]: halo plane z into slot (z + 4) % 4
         const int zz = wrap_any(z, g.nz);
         unsigned char* dst = halo + ((z + 4) & 3) * kSlotB;
         // one (channel, y row) per step: the 8 interior voxels as one 16-byte load (x0 and
         // nx are multiples of 8), the two periodic edge voxels as single loads
-        for (int e = t; e < 16 * HYC; e += 128) {
+        for (int e = t; e < CIN * HYC; e += 128) {
             const int yh = e % HYC, ci = e / HYC;
             const long long row = (long long)ci * g.N + (long long)g.nx * (wrap_any(y0 + yh - 1, g.ny) + (long long)g.ny * zz);
             const uint4 mid = *reinterpret_cast<const uint4*>(inb + row + x0);
@@ -429,9 +445,9 @@ __global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restri
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
-    float bs[16];
+    float bs[COUT];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) bs[c] = bias[c];
+    for (int c = 0; c < COUT; ++c) bs[c] = bias[c];
     const int m = warp * 32 + lane, xl = m & (CX - 1), yl = m / CX;
     uint32_t phase = 0;
     bool bad = false;
@@ -460,9 +476,13 @@ __global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restri
         const int y = y0 + yl;
         if (y < g.ny) {
             const long long v = (x0 + xl) + (long long)g.nx * (y + (long long)g.ny * z);
-            __nv_bfloat16* ob = out + (long long)b * 16 * g.N + v;
+            TO* ob = out + (long long)b * COUT * g.N + v;
 #pragma unroll
-            for (int c = 0; c < 16; ++c) ob[(long long)c * g.N] = __float2bfloat16(fmaxf(__uint_as_float(r[c]) + bs[c], 0.f));
+            for (int c = 0; c < COUT; ++c) {
+                float o = __uint_as_float(r[c]) + bs[c];
+                if (RELU) o = fmaxf(o, 0.f);
+                stf(ob + (long long)c * g.N, o);
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
@@ -482,17 +502,18 @@ __global__ void __launch_bounds__(128) k_conv16_tc(const __nv_bfloat16* __restri
     }
 }
 
-bool conv16_tc_ok(const Grid& g, int B) {
+bool conv_tc_ok(const Grid& g, int B) {
     if (g.nx % CX != 0 || B > 65535) return false;
     const long long nblk = (long long)(g.nx / CX) * ((g.ny + CY - 1) / CY) * ((g.nz + CZ - 1) / CZ);
     return nblk <= 0x7fffffffLL;
 }
 
-int launch_conv16_tc(const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias, __nv_bfloat16* out,
-                     const Grid& g, int B, int* err, cudaStream_t st) {
+template <int CIN, int COUT, bool RELU, typename TO>
+int launch_conv_tc(const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias, TO* out, const Grid& g, int B,
+                   int* err, cudaStream_t st) {
     const int tiles_y = (g.ny + CY - 1) / CY;
     const long long nblk = (long long)(g.nx / CX) * tiles_y * ((g.nz + CZ - 1) / CZ);
-    k_conv16_tc<<<dim3((unsigned)nblk, B), 128, kConvTcSmem, st>>>(in, W, bias, out, g, tiles_y, err);
+    k_conv_tc<CIN, COUT, RELU, TO><<<dim3((unsigned)nblk, B), 128, kConvTcSmem, st>>>(in, W, bias, out, g, tiles_y, err);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
 }
@@ -503,7 +524,7 @@ struct qg_learned_s {
     DevBuf master, adam_m, adam_v, grad, wbf, wtbf;  // params FP32 / BF16, transposed BF16 weights
     DevBuf act, dact, part, small, loss_acc;         // activations, gradients, partials, scratch
     int step = 0;
-    bool tensor_cores = true;  // the 16 -> 16 forward layers on tcgen05 where the grid allows
+    bool tensor_cores = true;  // the forward layers on tcgen05 where the grid allows
 };
 
 namespace {
@@ -531,16 +552,20 @@ int forward(qg_learned L, const Grid& g, int B, cudaStream_t st, __nv_bfloat16**
     *pout = p;
     const __nv_bfloat16* W = L->wbf.as<__nv_bfloat16>();
     const float* P = L->master.as<float>();  // biases are read in FP32
+    if (L->tensor_cores && conv_tc_ok(g, B)) {
+        // every layer on tcgen05 (16 x 16 channel MMAs; layer 1 pads its 2 input channels,
+        // layer 4 its 1 output channel)
+        int* err = L->ctx->dev_status;
+        QG_TRY((launch_conv_tc<2, 16, true>(a0, W + woff(0), P + woff(0) + wcount(0), a1, g, B, err, st)));
+        QG_TRY((launch_conv_tc<16, 16, true>(a1, W + woff(1), P + woff(1) + wcount(1), a2, g, B, err, st)));
+        QG_TRY((launch_conv_tc<16, 16, true>(a2, W + woff(2), P + woff(2) + wcount(2), a3, g, B, err, st)));
+        QG_TRY((launch_conv_tc<16, 1, false>(a3, W + woff(3), P + woff(3) + wcount(3), p, g, B, err, st)));
+        return QG_OK;
+    }
     const dim3 grid(g.tx * g.ty * g.tz, B);
     k_conv_fwd<2, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a0, W + woff(0), P + woff(0) + wcount(0), a1, nullptr, g);
-    if (L->tensor_cores && conv16_tc_ok(g, B)) {
-        int* err = L->ctx->dev_status;
-        QG_TRY(launch_conv16_tc(a1, W + woff(1), P + woff(1) + wcount(1), a2, g, B, err, st));
-        QG_TRY(launch_conv16_tc(a2, W + woff(2), P + woff(2) + wcount(2), a3, g, B, err, st));
-    } else {
-        k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a1, W + woff(1), P + woff(1) + wcount(1), a2, nullptr, g);
-        k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a2, W + woff(2), P + woff(2) + wcount(2), a3, nullptr, g);
-    }
+    k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a1, W + woff(1), P + woff(1) + wcount(1), a2, nullptr, g);
+    k_conv_fwd<16, 16, true, __nv_bfloat16, __nv_bfloat16><<<grid, TV, 0, st>>>(a2, W + woff(2), P + woff(2) + wcount(2), a3, nullptr, g);
     k_conv_fwd<16, 1, false, __nv_bfloat16, float><<<grid, TV, 0, st>>>(a3, W + woff(3), P + woff(3) + wcount(3), p, nullptr, g);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;

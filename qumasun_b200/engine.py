@@ -389,9 +389,31 @@ class LearnedPreconditioner:
               "qg_learned_get_params")
         return p
 
+    @staticmethod
+    def _check(grid, R, V, **blocks):
+        """The network reads R (ns, nx*ny*nz) and V (nx*ny*nz) and reads or writes the
+        other blocks whole: contiguous float64 CUDA tensors on one device, or a TypeError
+        / ValueError before the library is called."""
+        import torch
+        N = int(grid[0]) * int(grid[1]) * int(grid[2])
+        for name, T in (("R", R), ("V", V), *blocks.items()):
+            if not isinstance(T, torch.Tensor) or not T.is_cuda or T.dtype != torch.float64:
+                raise TypeError(f"{name} must be a float64 CUDA tensor")
+            if not T.is_contiguous():
+                raise ValueError(f"{name} must be contiguous")
+            if T.device != R.device:
+                raise ValueError(f"{name} is on {T.device}, R on {R.device}")
+        if R.dim() != 2 or R.shape[1] != N:
+            raise ValueError(f"R has shape {tuple(R.shape)}, expected (ns, {N})")
+        if V.numel() != N:
+            raise ValueError(f"V has {V.numel()} elements, expected {N}")
+        for name, T in blocks.items():
+            if T.shape != R.shape:
+                raise ValueError(f"{name} has shape {tuple(T.shape)}, R {tuple(R.shape)}")
+
     def set_tensor_cores(self, on: bool):
-        """Run the two 16 -> 16 forward layers on the tensor cores (the default, where
-        nx is a multiple of 8) or on the CUDA-core kernel."""
+        """Run the forward layers on the tensor cores (the default, where nx is a
+        multiple of 8) or on the CUDA-core kernels."""
         check(lib().qg_learned_set_tensor_cores(self.h, 1 if on else 0), "qg_learned_set_tensor_cores")
 
     def apply(self, grid, R, V, vscale, out=None, accumulate=False):
@@ -399,6 +421,7 @@ class LearnedPreconditioner:
         import torch
         if out is None:
             out = torch.zeros_like(R)
+        self._check(grid, R, V, out=out)
         self.ctx.use_torch_stream()
         check(lib().qg_learned_apply_d(self.h, grid[0], grid[1], grid[2], R.shape[0], C.c_void_p(R.data_ptr()),
                                        R.shape[1], C.c_void_p(V.data_ptr()), float(vscale), C.c_void_p(out.data_ptr()),
@@ -407,6 +430,7 @@ class LearnedPreconditioner:
 
     def gradient(self, grid, R, V, vscale, Y):
         """(loss, gradient) of one batch on the device (FP32 gradient, host)."""
+        self._check(grid, R, V, Y=Y)
         g = np.zeros(self.n_params, dtype=np.float32)
         loss = C.c_double()
         self.ctx.use_torch_stream()
@@ -417,6 +441,7 @@ class LearnedPreconditioner:
         return loss.value, g
 
     def train_step(self, grid, R, V, vscale, Y, lr):
+        self._check(grid, R, V, Y=Y)
         loss = C.c_double()
         self.ctx.use_torch_stream()
         check(lib().qg_learned_train_step(self.h, grid[0], grid[1], grid[2], R.shape[0], C.c_void_p(R.data_ptr()),

@@ -116,9 +116,9 @@ def test_learned_block_never_worse_than_kinetic(cuda_ctx):
 
 
 def test_tensor_core_layers_match_cuda_core_layers(cuda_ctx):
-    """The two 16 -> 16 forward layers on tcgen05 (halo planes in shared memory, one MMA
-    per tap) against the CUDA-core kernel on the same network and states: the same
-    output up to the order of the FP32 sums and the BF16 rounding of the activations.
+    """The forward layers on tcgen05 (halo planes in shared memory, one MMA per tap)
+    against the CUDA-core kernels on the same network and states: the same output up to
+    the order of the FP32 sums and the BF16 rounding of the activations.
     The grid has several column blocks in x and y, a partial y block (40 = 2 x 16 + 8)
     and a partial z slab (20 = 2 x 8 + 4)."""
     import torch
@@ -154,3 +154,28 @@ def test_forward_without_tensor_core_grid_matches_oracle(cuda_ctx):
     nn.close()
     ref = NN.apply(P, grid, R, V, 4.0)
     assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 5e-3
+
+
+def test_network_rejects_bad_tensors_before_the_library(cuda_ctx):
+    """float32, non-contiguous, wrongly sized or host tensors raise in Python: the
+    kernels would otherwise read or write past them."""
+    import torch
+    from qumasun_b200 import LearnedPreconditioner
+    grid = (16, 12, 8)
+    N = 16 * 12 * 8
+    R = torch.zeros(2, N, dtype=torch.float64, device="cuda")
+    V = torch.zeros(N, dtype=torch.float64, device="cuda")
+    nn = LearnedPreconditioner(cuda_ctx)
+    with pytest.raises(TypeError):
+        nn.apply(grid, R.float(), V, 4.0)
+    with pytest.raises(TypeError):
+        nn.apply(grid, R.cpu(), V, 4.0)
+    with pytest.raises(ValueError):
+        nn.apply(grid, torch.zeros(N, 2, dtype=torch.float64, device="cuda").t(), V, 4.0)
+    with pytest.raises(ValueError):
+        nn.apply(grid, R[:, : N - 8].contiguous(), V, 4.0)
+    with pytest.raises(ValueError):
+        nn.apply(grid, R, V[: N - 1], 4.0)
+    with pytest.raises(ValueError):
+        nn.gradient(grid, R, V, 4.0, torch.zeros(3, N, dtype=torch.float64, device="cuda"))
+    nn.close()
