@@ -125,6 +125,16 @@ __global__ void k_scale_cols(double* __restrict__ A, double* __restrict__ B, lon
     }
 }
 
+// dst_j = f_j src_j: the copy of a rotated block and its normalisation in one pass (the
+// same product as scaling the copy in place)
+__global__ void k_scale_copy(double* __restrict__ dst, const double* __restrict__ src, long long ld, long long N,
+                             const double* __restrict__ f) {
+    const int j = blockIdx.y;
+    const double c = f[j];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        dst[(long long)j * ld + i] = src[(long long)j * ld + i] * c;
+}
+
 // f[j] = 1 / sqrt(norm2[j] * dV)   (Normalize, vecmath.h:128-133)
 __global__ void k_inv_norm(const double* __restrict__ norm2, double dV, int n, double* __restrict__ f) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -531,6 +541,19 @@ struct Solver {
         coldot(A, A, 1.0, nr_d);
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(nr_d, dV, n, f_d);
         scale_cols(A, B);
+    }
+
+    // dst = src scaled by f_d, state by state
+    void scale_copy(double* dst, const double* src) {
+        dim3 g((unsigned)std::min<long long>((L + 255) / 256, 64), n);
+        k_scale_copy<<<g, 256, 0, st>>>(dst, src, L, L, f_d);
+    }
+
+    // dst = src / sqrt(|src_j|^2 dV): the copy of a rotated block and its normalisation
+    void normalize_from(double* dst, const double* src) {
+        coldot(src, src, 1.0, nr_d);
+        k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(nr_d, dV, n, f_d);
+        scale_copy(dst, src);
     }
 
     void residual() {
@@ -947,13 +970,11 @@ int run_lobpcg(qg_hamiltonian h, const qg_lobpcg_options* opt, int n, int comps,
             }
             continue;
         }
-        QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
-        QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         tm.mark(4, st);
         k_inv_norm<<<(n + 127) / 128, 128, 0, st>>>(s.nr_d, s.dV, n, s.f_d);  // norms of x' taken above
-        s.scale_cols(s.x, nullptr);
+        s.scale_copy(s.x, s.Tx);  // x = x' / |x'|, copy and scaling in one pass
         if (next_update) QG_CUDA_TRY(cudaMemcpyAsync(s.fx_d, s.f_d, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        s.normalize(s.p, nullptr);
+        s.normalize_from(s.p, s.Tp);
         if (next_update) {
             QG_CUDA_TRY(cudaMemcpyAsync(s.fp_d, s.f_d, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
             s.have_update = true;
@@ -1328,11 +1349,9 @@ int run_lobpcg_zk(qg_hamiltonian h, const qg_lobpcg_options* opt, int nk, const 
         if (!two) QG_TRY(rot_block(s.p, Mall + 4 * nb, g, s.Tp, 1.0));
         QG_CUDA_TRY(cudaMemcpyAsync(s.Tx, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         QG_TRY(rot_block(s.x, Mall, g, s.Tx, 1.0));
-        QG_CUDA_TRY(cudaMemcpyAsync(s.x, s.Tx, blk_bytes, cudaMemcpyDeviceToDevice, st));
-        QG_CUDA_TRY(cudaMemcpyAsync(s.p, s.Tp, blk_bytes, cudaMemcpyDeviceToDevice, st));
         tm.mark(4, st);
-        s.normalize(s.x, nullptr);
-        s.normalize(s.p, nullptr);
+        s.normalize_from(s.x, s.Tx);
+        s.normalize_from(s.p, s.Tp);
         tm.mark(0, st);
         QG_TRY(applyH(s.x, s.Ax));
         QG_TRY(applyH(s.p, s.Ap));
