@@ -309,7 +309,8 @@ __global__ void k_scale_f(float* __restrict__ x, long long n, const double* __re
 
 // ---------------------------------------------------------------------------
 // The network layers on the 5th-generation tensor cores (sm_100a).
-// One CTA (4 warps) owns a column block of CX x CY voxels of one state and marches CZ
+// One CTA (4 warps) owns a column block of CX x CY voxels of one state (two groups of 8
+// x-voxels, each one M = 128 MMA with its own 16-column accumulator) and marches CZ
 // planes in z. The input's halo planes (CX+2 x CY+2 voxels) sit in shared memory split
 // into two 8-channel halves, each voxel's 8 channels one 16-byte row, so that operand A
 // of one tap -- 128 voxels (x fastest) x 16 input channels -- is the canonical K-major
@@ -327,13 +328,14 @@ __global__ void k_scale_f(float* __restrict__ x, long long n, const double* __re
 // different order (per tap on the tensor cores).
 using namespace qg::tc;
 
-constexpr int CX = 8, CY = 16, CZ = 8;          // voxels of a CTA's column block; z planes per CTA
+constexpr int CX = 16, CY = 16, CZ = 8;         // voxels of a CTA's column block; z planes per CTA
+constexpr int kGroupsX = CX / 8;                // M = 128 groups (8 x-voxels x 16 y rows) per plane
 constexpr int HXC = CX + 2, HYC = CY + 2;
-constexpr int kHalfB = HXC * HYC * 16;          // one 8-channel half of a halo plane (2880 B)
+constexpr int kHalfB = HXC * HYC * 16;          // one 8-channel half of a halo plane (5184 B)
 constexpr int kSlotB = 2 * kHalfB;              // one halo plane
 constexpr int kSlots = 4;
 constexpr int kWB = 27 * 512;                   // weights, bf16 [tap][half][co][8]
-// shared memory: the halo ring, the weights, the mbarrier and the TMEM address (36.9 KB;
+// shared memory: the halo ring, the weights, the mbarrier and the TMEM address (54 KB;
 // a tap's operand reaches at most the end of the ring)
 constexpr int kConvTcSmem = kSlots * kSlotB + kWB + 64;
 constexpr uint32_t kIdescConv = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
@@ -370,7 +372,8 @@ __device__ __forceinline__ int wrap_any(int i, int n) {
 // out (B x COUT x N) = act(conv(in (B x CIN x N)) + bias); W bf16 [COUT][CIN][27];
 // CIN, COUT <= 16 (the MMA is always 16 x 16 per tap: missing input channels are zero
 // in the halo, missing output channels have zero weights and are not stored). Grid:
-// x = (x block, y block, z slab), y = state. Requires nx % CX == 0.
+// x = (x block, y block, z slab), y = state. Requires nx % 8 == 0; in a last x block of
+// 8 voxels the second group computes on periodic copies and stores nothing.
 template <int CIN, int COUT, bool RELU, typename TO>
 __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict__ in,
                                                  const __nv_bfloat16* __restrict__ W,
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
     uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + kWB);
     volatile uint32_t* tslot = reinterpret_cast<volatile uint32_t*>(bar + 1);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int txb = g.nx / CX;
+    const int txb = (g.nx + CX - 1) / CX;
     int blk = blockIdx.x;
     const int xb = blk % txb;
     blk /= txb;
@@ -416,21 +419,27 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
     }
     const __nv_bfloat16* inb = in + (long long)b * CIN * g.N;
     const int xl0 = wrap_any(x0 - 1, g.nx), xr0 = wrap_any(x0 + CX, g.nx);
+    int xm[kGroupsX];  // start of each 8-voxel interior run (periodic past nx; multiples of 8)
+#pragma unroll
+    for (int q = 0; q < kGroupsX; ++q) xm[q] = wrap_any(x0 + 8 * q, g.nx);
     auto load_plane = [&](int z) {  // z in [-1, nz]: halo plane z into slot (z + 4) % 4
         const int zz = wrap_any(z, g.nz);
         unsigned char* dst = halo + ((z + 4) & 3) * kSlotB;
-        // one (channel, y row) per step: the 8 interior voxels as one 16-byte load (x0 and
-        // nx are multiples of 8), the two periodic edge voxels as single loads
+        // one (channel, y row) per step: each run of 8 interior voxels as one 16-byte load
+        // (x0 and nx are multiples of 8), the two periodic edge voxels as single loads
         for (int e = t; e < CIN * HYC; e += 128) {
             const int yh = e % HYC, ci = e / HYC;
             const long long row = (long long)ci * g.N + (long long)g.nx * (wrap_any(y0 + yh - 1, g.ny) + (long long)g.ny * zz);
-            const uint4 mid = *reinterpret_cast<const uint4*>(inb + row + x0);
             __nv_bfloat16 vals[HXC];
             vals[0] = inb[row + xl0];
             vals[HXC - 1] = inb[row + xr0];
-            const __nv_bfloat16* mv = reinterpret_cast<const __nv_bfloat16*>(&mid);
 #pragma unroll
-            for (int i = 0; i < CX; ++i) vals[1 + i] = mv[i];
+            for (int q = 0; q < kGroupsX; ++q) {
+                const uint4 mid = *reinterpret_cast<const uint4*>(inb + row + xm[q]);
+                const __nv_bfloat16* mv = reinterpret_cast<const __nv_bfloat16*>(&mid);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) vals[1 + 8 * q + i] = mv[i];
+            }
             __nv_bfloat16* rowdst = reinterpret_cast<__nv_bfloat16*>(dst + (ci >> 3) * kHalfB + yh * HXC * 16) + (ci & 7);
 #pragma unroll
             for (int xh = 0; xh < HXC; ++xh) rowdst[xh * 8] = vals[xh];
@@ -448,7 +457,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
     float bs[COUT];
 #pragma unroll
     for (int c = 0; c < COUT; ++c) bs[c] = bias[c];
-    const int m = warp * 32 + lane, xl = m & (CX - 1), yl = m / CX;
+    const int m = warp * 32 + lane, xl = m & 7, yl = m >> 3;
     uint32_t phase = 0;
     bool bad = false;
     for (int z = z0; z < z1; ++z) {
@@ -456,9 +465,13 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
 #pragma unroll 1
             for (int tap = 0; tap < 27; ++tap) {
                 const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
-                const uint32_t a = hbase + (uint32_t)((((z - 1 + dz) + 4) & 3) * kSlotB + (dy * HXC + dx) * 16);
-                umma_conv(tmem, desc_nosw(a, kHalfB, HXC * 16), desc_nosw(wbase + tap * 512, 256, 128),
-                          tap ? 1u : 0u);
+                const uint64_t bd = desc_nosw(wbase + tap * 512, 256, 128);
+#pragma unroll
+                for (int q = 0; q < kGroupsX; ++q) {
+                    const uint32_t a =
+                        hbase + (uint32_t)((((z - 1 + dz) + 4) & 3) * kSlotB + (dy * HXC + dx + 8 * q) * 16);
+                    umma_conv(tmem + (uint32_t)(16 * q), desc_nosw(a, kHalfB, HXC * 16), bd, tap ? 1u : 0u);
+                }
             }
             umma_commit(bar);
         }
@@ -470,18 +483,22 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
         }
         phase ^= 1u;
         tc_fence_after();
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), r);
-        tmem_wait_ld();
         const int y = y0 + yl;
-        if (y < g.ny) {
-            const long long v = (x0 + xl) + (long long)g.nx * (y + (long long)g.ny * z);
-            TO* ob = out + (long long)b * COUT * g.N + v;
 #pragma unroll
-            for (int c = 0; c < COUT; ++c) {
-                float o = __uint_as_float(r[c]) + bs[c];
-                if (RELU) o = fmaxf(o, 0.f);
-                stf(ob + (long long)c * g.N, o);
+        for (int q = 0; q < kGroupsX; ++q) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * q), r);
+            tmem_wait_ld();
+            const int x = x0 + 8 * q + xl;
+            if (y < g.ny && x < g.nx) {
+                const long long v = x + (long long)g.nx * (y + (long long)g.ny * z);
+                TO* ob = out + (long long)b * COUT * g.N + v;
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) {
+                    float o = __uint_as_float(r[c]) + bs[c];
+                    if (RELU) o = fmaxf(o, 0.f);
+                    stf(ob + (long long)c * g.N, o);
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -503,8 +520,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
 }
 
 bool conv_tc_ok(const Grid& g, int B) {
-    if (g.nx % CX != 0 || B > 65535) return false;
-    const long long nblk = (long long)(g.nx / CX) * ((g.ny + CY - 1) / CY) * ((g.nz + CZ - 1) / CZ);
+    if (g.nx % 8 != 0 || B > 65535) return false;
+    const long long nblk = (long long)((g.nx + CX - 1) / CX) * ((g.ny + CY - 1) / CY) * ((g.nz + CZ - 1) / CZ);
     return nblk <= 0x7fffffffLL;
 }
 
@@ -512,7 +529,9 @@ template <int CIN, int COUT, bool RELU, typename TO>
 int launch_conv_tc(const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias, TO* out, const Grid& g, int B,
                    int* err, cudaStream_t st) {
     const int tiles_y = (g.ny + CY - 1) / CY;
-    const long long nblk = (long long)(g.nx / CX) * tiles_y * ((g.nz + CZ - 1) / CZ);
+    const long long nblk = (long long)((g.nx + CX - 1) / CX) * tiles_y * ((g.nz + CZ - 1) / CZ);
+    QG_CUDA_TRY(cudaFuncSetAttribute(k_conv_tc<CIN, COUT, RELU, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kConvTcSmem));
     k_conv_tc<CIN, COUT, RELU, TO><<<dim3((unsigned)nblk, B), 128, kConvTcSmem, st>>>(in, W, bias, out, g, tiles_y, err);
     QG_CUDA_TRY(cudaGetLastError());
     return QG_OK;
