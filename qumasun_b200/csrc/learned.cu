@@ -428,7 +428,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16* __restrict
         // one (channel, y row) per step: each run of 8 interior voxels as one 16-byte load
         // (x0 and nx are multiples of 8), the two periodic edge voxels as single loads
         for (int e = t; e < CIN * HYC; e += 128) {
-            const int yh = e % HYC, ci = e / HYC;
+            // channels on consecutive lanes: 8 lanes fill one voxel's 16-byte row
+            const int ci = e % CIN, yh = e / CIN;
             const long long row = (long long)ci * g.N + (long long)g.nx * (wrap_any(y0 + yh - 1, g.ny) + (long long)g.ny * zz);
             __nv_bfloat16 vals[HXC];
             vals[0] = inb[row + xl0];
